@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""Benchmark: GKeys/s of the B200 LSD radix sort against its HBM roofline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload u32_full] [--no-breakdown]
+
+A step is one full sort (upfront scan and histogram, every live onesweep
+pass, finishing kernels) of 2^28 keys already resident in HBM (1 GiB, far
+above the 126 MB L2); each step sorts its own unsorted copy. `value` is keys
+sorted per second over the K timed steps (CUDA events on the sort's stream,
+max over ranks). `e2e` times the host-slice C ABI call ts_sort_u32 on pinned
+host memory: the copy in, the sort and the copy out. `roofline` is the
+onesweep pass kernel: algorithmic bytes of one pass (read + write of every
+key) over its CUDA-event duration, against the measured HBM copy bandwidth.
+Under torchrun each rank sorts its own array (replicas: the crate's sort has
+no cross-device step).
+
+--impl reference times the crate's own algorithm on the host cores instead
+(its C restatement, sort_parallel on every core), on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "GKeys/s on 1 B200 vs HBM roofline, bit-exact; learned/batched vs plain radix"
+
+# name -> (key type, distribution, log2 n)
+WORKLOADS = {
+    "u32_full": ("u32", 0, 28), "u32_low_entropy": ("u32", 1, 28), "u32_range16": ("u32", 2, 28),
+    "i32_full": ("i32", 0, 28), "i32_low_entropy": ("i32", 1, 28), "i32_range16": ("i32", 2, 28),
+    "f32_full": ("f32", 0, 28), "f32_low_entropy": ("f32", 1, 28), "f32_range16": ("f32", 2, 28),
+    "u64_full": ("u64", 0, 27), "u64_low_entropy": ("u64", 1, 27), "u64_range16": ("u64", 2, 27),
+    "c1_u32_2p20": ("u32", 0, 20),
+}
+DIST_NAMES = ("full-entropy", "AND of 3 words", "16-bit range in the low bits")
+NP = {"u32": np.uint32, "i32": np.int32, "f32": np.float32, "u64": np.uint64}
+WIDTH = {"u32": 4, "i32": 4, "f32": 4, "u64": 8}
+
+
+def radix_keys_np(a: np.ndarray) -> np.ndarray:
+    """to_radix_key (src/key.rs:135-197) with numpy, for output checks."""
+    if a.dtype == np.float32:
+        b = a.view(np.uint32)
+        return b ^ ((b.view(np.int32) >> 31).view(np.uint32) | np.uint32(0x80000000))
+    if a.dtype == np.int32:
+        return a.view(np.uint32) ^ np.uint32(0x80000000)
+    return a
+
+
+def live_passes(keys: np.ndarray, width: int) -> int:
+    """Digits (8-bit) that some key does not share with the others."""
+    k = radix_keys_np(keys)
+    diff = np.bitwise_or.reduce(k ^ k[0])
+    live = 0
+    for d in range(width):
+        if (int(diff) >> (8 * d)) & 0xFF:
+            col = (k >> k.dtype.type(8 * d)) & k.dtype.type(0xFF)
+            live += int(np.any(col != col[0]))
+    return live
+
+
+def check_sorted(out: np.ndarray, ref_sum: int, ref_xor: int) -> bool:
+    k = radix_keys_np(out)
+    ok = bool(np.all(k[1:] >= k[:-1]))
+    b = out.view(np.uint64 if out.itemsize == 8 else np.uint32)
+    ok &= int(b.sum(dtype=np.uint64)) == ref_sum and int(np.bitwise_xor.reduce(b)) == ref_xor
+    return ok
+
+
+def checksums(a: np.ndarray) -> tuple[int, int]:
+    b = a.view(np.uint64 if a.itemsize == 8 else np.uint32)
+    return int(b.sum(dtype=np.uint64)), int(np.bitwise_xor.reduce(b))
+
+
+def gen(kind: str, dist: int, n: int, seed: int) -> np.ndarray:
+    from turbosort_b200 import workloads as W
+
+    return W.scale(kind, dist, n, seed=seed)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1].split()[0]))
+                    mx.append(float(f[2].split()[0]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(name)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_gbs() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(name: str):
+    """dram bytes per launch from a committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def cpu_sample_rate(kind: str, dist: int, n_full: int, budget_s: float, threads: int, seed: int):
+    """The oracle's sort_parallel (the crate's algorithm restated in C) on a
+    bounded sample of the workload: returns (GKeys/s, sample description)."""
+    from oracle import oracle as O
+
+    n = min(n_full, 1 << 24)
+    base = gen(kind, dist, n, seed)
+    work = base.copy()
+    O.sort_parallel_inplace(work, threads)  # warm-up
+    reps, total = 0, 0.0
+    while total < budget_s and reps < 50:
+        np.copyto(work, base)
+        t0 = time.perf_counter()
+        O.sort_parallel_inplace(work, threads)
+        total += time.perf_counter() - t0
+        reps += 1
+    return n * reps / total / 1e9, f"{reps} sorts of 2^{n.bit_length() - 1} keys of the same distribution"
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    kind, dist, lg = WORKLOADS[args.workload]
+    n_full = 1 << lg
+    threads = os.cpu_count() or 1
+    # size the sample so that warm-up + steps stay within ~2 minutes
+    probe_n = min(n_full, 1 << 22)
+    probe = gen(kind, dist, probe_n, 7)
+    t0 = time.perf_counter()
+    O.sort_parallel_inplace(probe, threads)
+    per_key = (time.perf_counter() - t0) / probe_n
+    n = n_full
+    while n > (1 << 20) and per_key * n * (args.steps + args.warmup) > 120.0:
+        n //= 2
+    base = gen(kind, dist, n, 0x9E3779B97F4A7C15)
+    work = base.copy()
+    for _ in range(args.warmup):
+        np.copyto(work, base)
+        O.sort_parallel_inplace(work, threads)
+    times = []
+    for _ in range(args.steps):
+        np.copyto(work, base)
+        t0 = time.perf_counter()
+        O.sort_parallel_inplace(work, threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = n * args.steps / total / 1e9
+    sample = f"{args.steps} sorts of 2^{n.bit_length() - 1} of the workload's keys (full workload 2^{lg})"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GKeys/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": kind,
+        "data": "synthetic (seeded xorshift64)",
+        "config": workload_config(args.workload),
+        "cpu_baseline": {"value": round(value, 4), "unit": "GKeys/s", "cores": threads, "kind": "port",
+                         "sample": sample,
+                         "what": "turbosort sort_parallel (src/parallel.rs) restated in C, pthreads on every core"},
+        "e2e": {"value": round(value, 4), "unit": "GKeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(name: str) -> dict:
+    kind, dist, lg = WORKLOADS[name]
+    return {"workload": f"plain LSD sort of 2^{lg} {kind} keys, {DIST_NAMES[dist]} (seeded xorshift64), 8-bit digits",
+            "name": name, "n": 1 << lg, "key_type": kind,
+            "l2": "inputs larger than L2 (1 GiB vs 126 MB); each step sorts its own unsorted copy",
+            "parallelism": "replicas"}
+
+
+def bench_device(ts, torch, ctx, kind, dist, lg, steps, warmup, seed, dist_mod, rank, world, timing=True):
+    n = 1 << lg
+    w = WIDTH[kind]
+    host = gen(kind, dist, n, seed)
+    s_ref, x_ref = checksums(host)
+    live = live_passes(host, w)
+    tdt = {"u32": torch.int32, "i32": torch.int32, "f32": torch.int32, "u64": torch.int64}[kind]
+    master = torch.from_numpy(host.view(np.int64 if w == 8 else np.int32)).to(f"cuda:{ctx.device}")
+    view_dt = {"u32": torch.uint32, "i32": torch.int32, "f32": torch.float32, "u64": torch.uint64}[kind]
+    copies = [master.clone() for _ in range(steps + warmup)]
+    del master
+    for i in range(warmup):
+        ts.sort(copies[i].view(view_dt), ctx)
+    torch.cuda.synchronize()
+    lib = ts.lib()
+    if dist_mod is not None:
+        dist_mod.barrier()
+    torch.cuda.synchronize()
+    ctx.reset_timings()
+    ctx.enable_timing(timing)
+    launches0 = lib.ts_ctx_launches(ctx.handle)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        ts.sort(copies[warmup + i].view(view_dt), ctx)
+    e1.record()
+    torch.cuda.synchronize()
+    if dist_mod is not None:
+        dist_mod.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = lib.ts_ctx_launches(ctx.handle) - launches0
+    tm = ctx.timings()
+    ctx.enable_timing(False)
+    ctx.synchronize()
+    out = copies[-1].cpu().numpy().view(NP[kind])
+    ok = check_sorted(out, s_ref, x_ref)
+    del copies
+    torch.cuda.empty_cache()
+    return {"ms_total": ms, "launches": launches, "timings": tm, "ok": ok, "live": live, "n": n, "w": w}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="u32_full", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-breakdown", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    import turbosort_b200 as ts
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist_mod = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    ctx = ts.Context(local)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+
+    kind, dist, lg = WORKLOADS[args.workload]
+    clocks = Clocks(local)
+    clocks.start()
+    r = bench_device(ts, torch, ctx, kind, dist, lg, args.steps, args.warmup, 0x9E3779B97F4A7C15 + rank, dist_mod,
+                     rank, world)
+    clk = clocks.stop()
+    ms = r["ms_total"]
+    if dist_mod is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+        ms = float(t.item())
+        okt = torch.tensor([0 if r["ok"] else 1], device=f"cuda:{local}")
+        dist_mod.all_reduce(okt, op=dist_mod.ReduceOp.MAX)
+        r["ok"] = okt.item() == 0
+    n, w, live = r["n"], r["w"], r["live"]
+    ms_step = ms / args.steps
+    value = world * n / (ms_step / 1e3) / 1e9
+
+    peak, peak_kind = measured_peak_gbs()
+    sweep_ms, sweep_count = r["timings"].get("onesweep", (0.0, 0))
+    live_launches = max(1, live * args.steps)
+    per_launch_ms = sweep_ms / live_launches if sweep_ms else None
+    pass_bytes = n * w * 2
+    achieved = pass_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None
+    sort_bytes = n * w * (2 * live + 1)
+    traffic = ncu_traffic(f"onesweep_{kind}_2p{lg}.txt")
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GKeys/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": kind, "data": "synthetic (seeded xorshift64 keys)",
+        "config": workload_config(args.workload),
+        "bit_exact_checks": "sorted + sum/xor of the multiset" if r["ok"] else "FAILED",
+        "roofline": {
+            "bound": "hbm", "kernel": "k_onesweep (one live digit pass)",
+            "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4) if achieved else None, "peak_source": peak_kind,
+            "traffic": traffic, "algorithmic_bytes_per_launch": pass_bytes,
+            "avg_launch_ms": round(per_launch_ms, 4) if per_launch_ms else None,
+            "live_passes": live,
+            "sort_bytes": sort_bytes,
+            "sort_achieved_gbs": round(sort_bytes / (ms_step / 1e3) / 1e9, 1),
+            "sort_frac": round(sort_bytes / (ms_step / 1e3) / 1e9 / peak, 4),
+        },
+        "kernel_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in r["timings"].items()},
+        "gpu_launches": int(r["launches"]),
+        "clocks": clk,
+    }
+
+    # end to end through the host-slice C ABI call, pinned host memory
+    if not args.no_e2e:
+        host = gen(kind, dist, n, 0x9E3779B97F4A7C15 + rank)
+        pinned = torch.empty(n * w, dtype=torch.uint8, pin_memory=True).numpy().view(NP[kind])
+        e_ms = []
+        for i in range(args.warmup + args.steps):
+            np.copyto(pinned, host)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ts.sort(pinned, ctx)
+            e1.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                e_ms.append(e0.elapsed_time(e1))
+        emax = sum(e_ms)
+        if dist_mod is not None:
+            t = torch.tensor([emax], dtype=torch.float64, device=f"cuda:{local}")
+            dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+            emax = float(t.item())
+        s_ref, x_ref = checksums(host)
+        line["e2e"] = {"value": round(world * n * args.steps / (emax / 1e3) / 1e9, 3), "unit": "GKeys/s",
+                       "h2d_bytes_per_step": n * w, "d2h_bytes_per_step": n * w,
+                       "ms_per_step": round(emax / args.steps, 3),
+                       "call": f"ts_sort_{kind} on pinned host memory",
+                       "bit_exact_checks": "sorted + sum/xor" if check_sorted(pinned, s_ref, x_ref) else "FAILED"}
+        del pinned
+
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, sample = cpu_sample_rate(kind, dist, n, 15.0, threads, 0x9E3779B97F4A7C15)
+        line["cpu_baseline"] = {"value": round(rate, 4), "unit": "GKeys/s", "cores": threads, "kind": "port",
+                                "sample": sample,
+                                "what": "turbosort sort_parallel (src/parallel.rs) restated in C, pthreads"}
+
+    if not args.no_breakdown:
+        bd = {}
+        for name in [k for k in WORKLOADS if k != args.workload and k != "c1_u32_2p20"] + ["c1_u32_2p20"]:
+            k2, d2, l2 = WORKLOADS[name]
+            rr = bench_device(ts, torch, ctx, k2, d2, l2, max(3, args.steps // 2), 3, 0x1234 + rank, None, rank,
+                              world)
+            st = rr["ms_total"] / max(3, args.steps // 2)
+            sb = rr["n"] * rr["w"] * (2 * rr["live"] + 1)
+            ow = rr["timings"].get("onesweep", (0.0, 0))[0] / max(1, rr["live"] * max(3, args.steps // 2))
+            bd[name] = {"gkeys_s": round(rr["n"] / (st / 1e3) / 1e9, 2), "ms": round(st, 4), "live_passes": rr["live"],
+                        "sort_frac": round(sb / (st / 1e3) / 1e9 / peak, 3),
+                        "pass_frac": round(rr["n"] * rr["w"] * 2 / (ow / 1e3) / 1e9 / peak, 3) if ow else None,
+                        "ok": rr["ok"]}
+        line["breakdown"] = bd
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist_mod is not None:
+        dist_mod.barrier()
+        dist_mod.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+/*
+ * turbosort.h — C ABI of the B200 radix sort (libturbosort_b200.so).
+ *
+ * Drop-in for the sort path of the turbosort crate (Rust, 0.2.2). Each entry
+ * point names the crate function it replaces (file:line in the crate). The
+ * crate's generic functions over its ten SortableKey types (src/key.rs:64-77)
+ * become one symbol per type, suffixed u8 u16 u32 u64 i8 i16 i32 i64 f32 f64,
+ * which is what an `extern "C"` binding per type would call. Floats sort in
+ * total_cmp order (src/key.rs:162-197): -NaN < -inf < ... < -0.0 < +0.0 < ...
+ * < +inf < +NaN, and every bit pattern comes back unchanged.
+ *
+ * Host entry points take host slices, as the crate does: they copy to the
+ * device, sort there and copy back before returning. `_dev` entry points take
+ * device pointers and only enqueue work on the context's stream; call
+ * ts_ctx_synchronize() to wait and collect errors.
+ *
+ * Panics of the crate become status codes: a buffer shorter than the slice
+ * (src/dispatch.rs:78-83) is TS_ERR_BUFFER_TOO_SMALL, an apply_order length
+ * mismatch (src/by_key.rs:137-141) is TS_ERR_LENGTH_MISMATCH. A context is
+ * used by one host thread at a time.
+ */
+#ifndef TURBOSORT_H
+#define TURBOSORT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ts_status {
+    TS_OK = 0,
+    TS_ERR_BUFFER_TOO_SMALL = 1, /* src/dispatch.rs:78-83, src/radix/mod.rs:92-97 */
+    TS_ERR_LENGTH_MISMATCH = 2,  /* src/by_key.rs:137-141 */
+    TS_ERR_CUDA = 3,             /* a CUDA call failed; see ts_ctx_last_error */
+    TS_ERR_TIMEOUT = 4,          /* a bounded device wait ran out; the output is not valid */
+    TS_ERR_OOM = 5,              /* device memory could not be reserved */
+    TS_ERR_INVALID = 6,          /* a null context or pointer, or an unusable argument */
+    TS_ERR_NO_DEVICE = 7,        /* no CUDA device */
+    TS_ERR_TOO_LARGE = 8,        /* more than u32::MAX elements where positions are u32 */
+    TS_ERR_INTERNAL = 9          /* a device-side bounds check fired */
+} ts_status;
+
+typedef struct ts_ctx ts_ctx;
+
+/* Context: a CUDA stream plus device scratch that grows to the largest sort
+ * (like SortByKeyBuffer, src/by_key.rs:40-90) and is kept between calls. */
+ts_status ts_ctx_create(int device, ts_ctx **out);
+void ts_ctx_destroy(ts_ctx *ctx);
+/* Use `stream` (a cudaStream_t, or NULL for the legacy default stream)
+ * instead of the context's own stream. */
+ts_status ts_ctx_set_stream(ts_ctx *ctx, void *stream);
+void *ts_ctx_stream(ts_ctx *ctx);
+/* Wait for the context's stream; reports errors raised by kernels. */
+ts_status ts_ctx_synchronize(ts_ctx *ctx);
+/* Reserve scratch for `n` elements of `key_bytes`, with positions when
+ * `with_order` (SortByKeyBuffer::with_capacity, src/by_key.rs:74-81). */
+ts_status ts_ctx_reserve(ts_ctx *ctx, size_t n, size_t key_bytes, int with_order);
+/* Elements of `key_bytes` the context can sort without growing
+ * (SortByKeyBuffer::capacity, src/by_key.rs:84-90). */
+size_t ts_ctx_capacity(const ts_ctx *ctx, size_t key_bytes, int with_order);
+const char *ts_ctx_last_error(const ts_ctx *ctx);
+const char *ts_status_str(ts_status s);
+
+/* Per-kernel timing with CUDA events on the context's stream (off by default).
+ * ts_ctx_timings fills up to `max` (name, total ms, count) triples, sorted by
+ * name, and returns how many kernels were seen; it waits for the stream. */
+ts_status ts_ctx_enable_timing(ts_ctx *ctx, int on);
+int ts_ctx_timings(ts_ctx *ctx, char (*names)[32], double *ms, long *counts, int max);
+void ts_ctx_reset_timings(ts_ctx *ctx);
+/* Kernels this context has launched so far (all entry points). */
+unsigned long long ts_ctx_launches(const ts_ctx *ctx);
+
+#define TS_DECLARE_SORTS(SUF, T)                                                                     \
+    /* turbosort::sort (src/lib.rs:99): ascending, in place. */                                       \
+    ts_status ts_sort_##SUF(ts_ctx *ctx, T *data, size_t n);                                          \
+    /* turbosort::sort_with_buffer (src/lib.rs:122): the buffer must hold n elements. */              \
+    ts_status ts_sort_with_buffer_##SUF(ts_ctx *ctx, T *data, size_t n, T *buf, size_t buf_len);      \
+    /* turbosort::sort_parallel (src/lib.rs:224): the same device sort. */                            \
+    ts_status ts_sort_parallel_##SUF(ts_ctx *ctx, T *data, size_t n);                                 \
+    /* sort_by_key_with_buffer + SortByKeyBuffer::order (src/by_key.rs:175-233, :108): the keys the   \
+     * closure returned, one per element; writes order[i] = source index of output slot i (stable).   \
+     * Returns TS_ERR_TOO_LARGE above u32::MAX elements, where the crate leaves order() empty. */      \
+    ts_status ts_sort_keys_order_##SUF(ts_ctx *ctx, const T *keys, size_t n, uint32_t *order);        \
+    /* Device-resident forms; enqueued on the context's stream. */                                    \
+    ts_status ts_sort_dev_##SUF(ts_ctx *ctx, T *d_data, size_t n);                                    \
+    ts_status ts_sort_dev_with_buffer_##SUF(ts_ctx *ctx, T *d_data, size_t n, T *d_buf, size_t buf_len); \
+    ts_status ts_sort_keys_order_dev_##SUF(ts_ctx *ctx, const T *d_keys, size_t n, uint32_t *d_order);
+
+TS_DECLARE_SORTS(u8, uint8_t)
+TS_DECLARE_SORTS(u16, uint16_t)
+TS_DECLARE_SORTS(u32, uint32_t)
+TS_DECLARE_SORTS(u64, uint64_t)
+TS_DECLARE_SORTS(i8, int8_t)
+TS_DECLARE_SORTS(i16, int16_t)
+TS_DECLARE_SORTS(i32, int32_t)
+TS_DECLARE_SORTS(i64, int64_t)
+TS_DECLARE_SORTS(f32, float)
+TS_DECLARE_SORTS(f64, double)
+
+/* SortByKeyBuffer::apply_order (src/by_key.rs:136-144, :315-334): position i of
+ * `data` (n elements of `elem_size` bytes) gets the element that was at
+ * order[i]. `order` must be a permutation of 0..n. */
+ts_status ts_apply_order(ts_ctx *ctx, void *data, size_t n, size_t elem_size, const uint32_t *order,
+                         size_t order_len);
+ts_status ts_apply_order_dev(ts_ctx *ctx, void *d_data, size_t n, size_t elem_size, const uint32_t *d_order,
+                             size_t order_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TURBOSORT_H */

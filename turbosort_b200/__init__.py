@@ -1,0 +1,355 @@
+"""turbosort_b200 — the turbosort crate's sort API on a B200, over its C ABI.
+
+Mirrors the crate's public functions (src/lib.rs) for numpy arrays (host
+slices: copied to the GPU, sorted there, copied back) and CUDA torch tensors
+(device slices: sorted in place on the context's stream):
+
+    sort(a)                      src/lib.rs:99
+    sort_with_buffer(a, buf)     src/lib.rs:122   ValueError "buffer too small: need N, got M"
+    sort_parallel(a)             src/lib.rs:224
+    sort_by_key(items, key)      src/lib.rs:152   stable; key called once per element
+    sort_by_key_with_buffer(items, buffer, key)   src/lib.rs:196
+    SortByKeyBuffer.order() / .apply_order(other) / .capacity()   src/by_key.rs:51-145
+
+Every call goes through libturbosort_b200.so (include/turbosort.h); there is
+no CPU fallback: without the library or a CUDA device the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+__all__ = [
+    "Context", "SortByKeyBuffer", "TurbosortError", "apply_order", "default_context", "lib", "sort",
+    "sort_by_key", "sort_by_key_with_buffer", "sort_parallel", "sort_with_buffer", "TYPES",
+]
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libturbosort_b200.so")
+
+TYPES = ("u8", "u16", "u32", "u64", "i8", "i16", "i32", "i64", "f32", "f64")
+_NP = {
+    "u8": np.uint8, "u16": np.uint16, "u32": np.uint32, "u64": np.uint64,
+    "i8": np.int8, "i16": np.int16, "i32": np.int32, "i64": np.int64,
+    "f32": np.float32, "f64": np.float64,
+}
+_TORCH_NAME = {
+    "uint8": "u8", "uint16": "u16", "uint32": "u32", "uint64": "u64", "int8": "i8", "int16": "i16",
+    "int32": "i32", "int64": "i64", "float32": "f32", "float64": "f64",
+}
+
+TS_OK = 0
+STATUS = {
+    1: "TS_ERR_BUFFER_TOO_SMALL", 2: "TS_ERR_LENGTH_MISMATCH", 3: "TS_ERR_CUDA", 4: "TS_ERR_TIMEOUT",
+    5: "TS_ERR_OOM", 6: "TS_ERR_INVALID", 7: "TS_ERR_NO_DEVICE", 8: "TS_ERR_TOO_LARGE", 9: "TS_ERR_INTERNAL",
+}
+
+
+class TurbosortError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C ABI library. Raises if it has not been built."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} is missing: build it with `python -m turbosort_b200.build` (nvcc, sm_100a)")
+            L = ctypes.CDLL(LIB_PATH)
+            vp, sz, i, st = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_int
+            L.ts_ctx_create.argtypes = [i, ctypes.POINTER(vp)]
+            L.ts_ctx_create.restype = st
+            L.ts_ctx_destroy.argtypes = [vp]
+            L.ts_ctx_destroy.restype = None
+            L.ts_ctx_set_stream.argtypes = [vp, vp]
+            L.ts_ctx_set_stream.restype = st
+            L.ts_ctx_stream.argtypes = [vp]
+            L.ts_ctx_stream.restype = vp
+            L.ts_ctx_synchronize.argtypes = [vp]
+            L.ts_ctx_synchronize.restype = st
+            L.ts_ctx_reserve.argtypes = [vp, sz, sz, i]
+            L.ts_ctx_reserve.restype = st
+            L.ts_ctx_capacity.argtypes = [vp, sz, i]
+            L.ts_ctx_capacity.restype = sz
+            L.ts_ctx_last_error.argtypes = [vp]
+            L.ts_ctx_last_error.restype = ctypes.c_char_p
+            L.ts_status_str.argtypes = [st]
+            L.ts_status_str.restype = ctypes.c_char_p
+            L.ts_ctx_enable_timing.argtypes = [vp, i]
+            L.ts_ctx_enable_timing.restype = st
+            L.ts_ctx_timings.argtypes = [vp, vp, vp, vp, i]
+            L.ts_ctx_timings.restype = i
+            L.ts_ctx_reset_timings.argtypes = [vp]
+            L.ts_ctx_reset_timings.restype = None
+            for t in TYPES:
+                for name, args in (
+                    ("ts_sort_", [vp, vp, sz]),
+                    ("ts_sort_with_buffer_", [vp, vp, sz, vp, sz]),
+                    ("ts_sort_parallel_", [vp, vp, sz]),
+                    ("ts_sort_keys_order_", [vp, vp, sz, vp]),
+                    ("ts_sort_dev_", [vp, vp, sz]),
+                    ("ts_sort_dev_with_buffer_", [vp, vp, sz, vp, sz]),
+                    ("ts_sort_keys_order_dev_", [vp, vp, sz, vp]),
+                ):
+                    f = getattr(L, name + t)
+                    f.argtypes = args
+                    f.restype = st
+            L.ts_apply_order.argtypes = [vp, vp, sz, sz, vp, sz]
+            L.ts_apply_order.restype = st
+            L.ts_apply_order_dev.argtypes = [vp, vp, sz, sz, vp, sz]
+            L.ts_apply_order_dev.restype = st
+            _lib = L
+        return _lib
+
+
+class Context:
+    """A CUDA stream plus device scratch that grows to the largest sort."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        self._check(lib().ts_ctx_create(device, ctypes.byref(self._h)))
+        self.device = device
+
+    def _check(self, status: int) -> None:
+        if status != TS_OK:
+            msg = lib().ts_ctx_last_error(self._h).decode() if getattr(self, "_h", None) else ""
+            if status == 1:
+                raise ValueError(msg)
+            if status == 2:
+                raise ValueError(msg)
+            raise TurbosortError(status, msg or lib().ts_status_str(status).decode())
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().ts_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        self._check(lib().ts_ctx_set_stream(self._h, stream_handle or None))
+
+    def synchronize(self) -> None:
+        self._check(lib().ts_ctx_synchronize(self._h))
+
+    def reserve(self, n: int, key_bytes: int, with_order: bool = False) -> None:
+        self._check(lib().ts_ctx_reserve(self._h, n, key_bytes, int(with_order)))
+
+    def capacity(self, key_bytes: int, with_order: bool = False) -> int:
+        return int(lib().ts_ctx_capacity(self._h, key_bytes, int(with_order)))
+
+    def enable_timing(self, on: bool = True) -> None:
+        self._check(lib().ts_ctx_enable_timing(self._h, int(on)))
+
+    def reset_timings(self) -> None:
+        lib().ts_ctx_reset_timings(self._h)
+
+    def timings(self) -> dict[str, tuple[float, int]]:
+        """{kernel group: (total ms, launches)} since the last reset."""
+        m = 64
+        names = (ctypes.c_char * 32 * m)()
+        ms = (ctypes.c_double * m)()
+        cnt = (ctypes.c_long * m)()
+        k = lib().ts_ctx_timings(self._h, names, ms, cnt, m)
+        return {bytes(names[i]).split(b"\0")[0].decode(): (ms[i], cnt[i]) for i in range(min(k, m))}
+
+
+_default: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    ctx = _default.get(device)
+    if ctx is None:
+        ctx = _default[device] = Context(device)
+    return ctx
+
+
+def _is_torch(a) -> bool:
+    return type(a).__module__.startswith("torch")
+
+
+def _type_of(a) -> str:
+    if _is_torch(a):
+        t = _TORCH_NAME.get(str(a.dtype).replace("torch.", ""))
+    else:
+        t = next((k for k, d in _NP.items() if a.dtype == np.dtype(d)), None)
+    if t is None:
+        raise TypeError(f"{a.dtype} is not one of the ten sortable types")
+    return t
+
+
+def _host_ptr(a: np.ndarray) -> int:
+    if not a.flags.c_contiguous:
+        raise ValueError("the slice must be contiguous")
+    if not a.flags.writeable:
+        raise ValueError("the slice must be writeable")
+    return a.ctypes.data
+
+
+def _dev(a) -> bool:
+    if _is_torch(a):
+        if not a.is_cuda:
+            raise ValueError("torch tensors must be on a CUDA device; pass numpy arrays for host slices")
+        if not a.is_contiguous():
+            raise ValueError("the slice must be contiguous")
+        return True
+    return False
+
+
+def sort(a, ctx: Context | None = None) -> None:
+    """Sort `a` in place, ascending in the crate's key order (src/lib.rs:99)."""
+    ctx = ctx or default_context(a.device.index if _is_torch(a) else 0)
+    t = _type_of(a)
+    if _dev(a):
+        ctx._check(getattr(lib(), f"ts_sort_dev_{t}")(ctx.handle, a.data_ptr(), a.numel()))
+    else:
+        ctx._check(getattr(lib(), f"ts_sort_{t}")(ctx.handle, _host_ptr(a), a.size))
+
+
+def sort_with_buffer(a, buf, ctx: Context | None = None) -> None:
+    """Sort with a caller-provided buffer of at least len(a) (src/lib.rs:122).
+    Raises ValueError("buffer too small: need N, got M") like the crate's panic."""
+    ctx = ctx or default_context(a.device.index if _is_torch(a) else 0)
+    t = _type_of(a)
+    if _type_of(buf) != t:
+        raise TypeError("the buffer's type differs from the slice's")
+    if _dev(a):
+        if not _dev(buf):
+            raise ValueError("a device slice needs a device buffer")
+        ctx._check(getattr(lib(), f"ts_sort_dev_with_buffer_{t}")(ctx.handle, a.data_ptr(), a.numel(),
+                                                                   buf.data_ptr(), buf.numel()))
+    else:
+        ctx._check(getattr(lib(), f"ts_sort_with_buffer_{t}")(ctx.handle, _host_ptr(a), a.size,
+                                                               buf.ctypes.data, buf.size))
+
+
+def sort_parallel(a, ctx: Context | None = None) -> None:
+    """The crate's multi-core sort (src/lib.rs:224): the same device sort here."""
+    ctx = ctx or default_context(a.device.index if _is_torch(a) else 0)
+    t = _type_of(a)
+    if _dev(a):
+        ctx._check(getattr(lib(), f"ts_sort_dev_{t}")(ctx.handle, a.data_ptr(), a.numel()))
+    else:
+        ctx._check(getattr(lib(), f"ts_sort_parallel_{t}")(ctx.handle, _host_ptr(a), a.size))
+
+
+def keys_order(keys, ctx: Context | None = None, out=None):
+    """The stable order of `keys` (one sortable key per element): out[i] is the
+    source index of output slot i (SortByKeyBuffer::order, src/by_key.rs:108)."""
+    ctx = ctx or default_context(keys.device.index if _is_torch(keys) else 0)
+    t = _type_of(keys)
+    if _dev(keys):
+        import torch
+
+        if out is None:
+            out = torch.empty(keys.numel(), dtype=torch.int32, device=keys.device)
+        ctx._check(getattr(lib(), f"ts_sort_keys_order_dev_{t}")(ctx.handle, keys.data_ptr(), keys.numel(),
+                                                                  out.data_ptr()))
+        return out
+    k = np.ascontiguousarray(keys)
+    if out is None:
+        out = np.empty(k.size, dtype=np.uint32)
+    ctx._check(getattr(lib(), f"ts_sort_keys_order_{t}")(ctx.handle, k.ctypes.data, k.size, out.ctypes.data))
+    return out
+
+
+def apply_order(data, order, ctx: Context | None = None) -> None:
+    """Put `data` in `order` in place: position i gets the element at order[i]."""
+    ctx = ctx or default_context(data.device.index if _is_torch(data) else 0)
+    if _is_torch(data):
+        _dev(data)
+        n = data.shape[0] if data.dim() else 0
+        elem = data.element_size() * (data[0].numel() if n else 1)
+        ctx._check(lib().ts_apply_order_dev(ctx.handle, data.data_ptr(), n, elem, order.data_ptr(), order.numel()))
+        return
+    n = data.shape[0] if data.ndim else 0
+    elem = data.itemsize * (int(np.prod(data.shape[1:])) if data.ndim > 1 else 1)
+    o = np.ascontiguousarray(order, dtype=np.uint32)
+    ctx._check(lib().ts_apply_order(ctx.handle, _host_ptr(data), n, elem, o.ctypes.data, o.size))
+
+
+def _key_array(items, key, dtype):
+    vals = [key(x) for x in items]  # exactly one call per element (src/lib.rs:165-166)
+    if dtype is None:
+        if vals and isinstance(vals[0], np.generic):
+            dtype = vals[0].dtype
+        elif vals and isinstance(vals[0], float):
+            dtype = np.float64
+        else:
+            dtype = np.int64
+    return np.asarray(vals, dtype=dtype)
+
+
+class SortByKeyBuffer:
+    """Reusable memory for sort_by_key_with_buffer (src/by_key.rs:51-145):
+    the device scratch of its own context, and the order of the last sort."""
+
+    def __init__(self, capacity: int = 0, key_bytes: int = 8, device: int = 0):
+        self.ctx = Context(device)
+        self._order = np.empty(0, dtype=np.uint32)
+        if capacity:
+            self.ctx.reserve(capacity, key_bytes, with_order=True)
+
+    def capacity(self, key_bytes: int = 8) -> int:
+        return self.ctx.capacity(key_bytes, with_order=True)
+
+    def order(self) -> np.ndarray:
+        """After a sort, position i of the sorted slice holds the element that
+        was at order()[i]. Empty before the first sort (src/by_key.rs:92-110)."""
+        return self._order
+
+    def apply_order(self, other, scratch=None) -> None:
+        """Put `other` in the order of the last sort (src/by_key.rs:136-144).
+        Raises ValueError on a length mismatch, as the crate panics."""
+        n = len(other)
+        if n != self._order.size:
+            raise ValueError("apply_order: the slice's length differs from the last sorted slice's")
+        if isinstance(other, np.ndarray) and other.dtype != object:
+            apply_order(other, self._order, self.ctx)
+        else:
+            moved = [other[int(i)] for i in self._order]
+            other[:] = moved
+        if scratch is not None:
+            scratch.clear()
+
+
+def sort_by_key_with_buffer(items, buffer: SortByKeyBuffer, key, dtype=None) -> None:
+    """Stable sort of `items` by key(x) (src/lib.rs:196, src/by_key.rs:175-235).
+    `items` is a list or a numpy array; key runs once per element on the host."""
+    keys = _key_array(items, key, dtype)
+    n = keys.size
+    if n < 2:
+        buffer._order = np.arange(n, dtype=np.uint32)
+        return
+    if n > 0xFFFFFFFF:
+        buffer._order = np.empty(0, dtype=np.uint32)  # order() is empty (src/by_key.rs:190-194)
+        idx = np.argsort(keys, kind="stable")
+        moved = [items[int(i)] for i in idx]
+        items[:] = moved
+        return
+    buffer._order = keys_order(keys, buffer.ctx)
+    buffer.apply_order(items)
+
+
+def sort_by_key(items, key, dtype=None) -> None:
+    """Stable sort by key, with a fresh buffer (src/lib.rs:152)."""
+    sort_by_key_with_buffer(items, SortByKeyBuffer(), key, dtype)

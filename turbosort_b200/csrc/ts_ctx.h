@@ -1,0 +1,73 @@
+// ts_ctx.h — the context behind the C ABI: one CUDA stream, grow-only device
+// scratch (the GPU counterpart of the crate's scratch buffers and of
+// SortByKeyBuffer, src/by_key.rs:51-90), the error word the kernels report
+// through, and optional per-kernel CUDA-event timing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/turbosort.h"
+
+namespace ts {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace ts
+
+struct ts_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // grow-only device buffers
+    ts::DevBuf keys, alt;          // staged keys and their ping-pong partner
+    ts::DevBuf vals0, vals1;       // positions ping-pong (sort_by_key)
+    ts::DevBuf order;              // the order of the last sort_by_key
+    ts::DevBuf meta;               // scan state, plan, histograms, scans, counters, carries
+    ts::DevBuf lookback;           // two look-back regions
+    ts::DevBuf gather;             // apply_order staging
+    uint32_t* d_error = nullptr;   // kernel-reported errors, read and cleared by the host
+
+    std::string last_error;
+    unsigned long long launches = 0;   // kernels this context has launched
+
+    // timing: named marks on the stream, folded into per-name totals on read
+    bool timing = false;
+    std::vector<std::pair<std::string, cudaEvent_t>> marks;
+    std::vector<cudaEvent_t> spare_events;
+    std::map<std::string, std::pair<double, long>> totals;
+};
+
+namespace ts {
+
+// Record a named mark: the time until the next mark is charged to `name`.
+void mark(ts_ctx* c, const char* name);
+// Fold the recorded marks into totals (synchronises on the last mark).
+void fold_marks(ts_ctx* c);
+
+ts_status fail(ts_ctx* c, ts_status s, const std::string& msg);
+ts_status cuda_fail(ts_ctx* c, cudaError_t e, const char* where);
+ts_status grow(ts_ctx* c, DevBuf& b, size_t bytes, const char* what);
+
+// Device sorts, enqueued on c->stream. The caller checks the error word.
+template <typename U, int XF>
+ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt);
+template <typename U, int XF>
+ts_status order_device(ts_ctx* c, const U* d_keys, size_t n, uint32_t* d_order);
+
+}  // namespace ts
+
+#define TS_CUDA(c, call)                                        \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return ts::cuda_fail((c), e_, #call); \
+    } while (0)

@@ -1,0 +1,231 @@
+// ts_engine.cuh — host-side drivers that enqueue one device sort.
+//
+// The tier choice follows the crate's dispatcher (src/dispatch.rs:31-111):
+// n <= 1 is a no-op; one-byte keys take the counting sort
+// (src/radix/mod.rs:123-164); short slices take the bitonic tier
+// (src/tiny.rs, src/small.rs, here up to 4096 keys); the rest runs the LSD
+// passes (src/radix/mod.rs:180-271). The presorted early-out
+// (src/presorted.rs:15-65) and the constant-digit skip are decided on the
+// device, so nothing in a sort waits on the host.
+#pragma once
+
+#include <algorithm>
+#include <type_traits>
+
+#include "ts_ctx.h"
+#include "ts_lsd.cuh"
+#include "ts_small.cuh"
+
+namespace ts {
+
+// Tile shapes per key width (threads x items per thread); 8-bit digits.
+template <typename U, bool PAIRS>
+struct LsdCfg {
+    static constexpr int BITS = 8;
+    static constexpr int THREADS = 512;
+    static constexpr int IPT = sizeof(U) == 8 ? 8 : (PAIRS ? 12 : 16);
+    static constexpr int TILE = THREADS * IPT;
+    static constexpr int RADIX = 1 << BITS;
+    static constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
+};
+
+// Layout of ctx->meta for one sort.
+struct MetaLayout {
+    size_t scan_off, plan_off, counters_off, hist_off, bins_off, carry_off, bytes;
+    static MetaLayout make(int nd, int radix, int launches) {
+        MetaLayout m{};
+        size_t o = 0;
+        m.scan_off = o;
+        o += 256;
+        m.plan_off = o;
+        o += 256;
+        m.counters_off = o;
+        o += ((size_t)launches * 4 + 255) / 256 * 256;
+        m.hist_off = o;
+        o += (size_t)nd * radix * 8;
+        m.bins_off = o;
+        o += (size_t)nd * radix * 8;
+        m.carry_off = o;
+        o += (size_t)2 * radix * 8;
+        m.bytes = o;
+        return m;
+    }
+    size_t zero_bytes() const { return bins_off; }  // scan state .. histograms
+};
+
+// Resident CTAs per SM for `kernel`, raising its dynamic shared memory limit
+// first when it needs more than the default 48 KB. Cached per kernel.
+int occupancy_of(const void* kernel, int threads, size_t smem);
+template <typename K>
+static int occupancy(ts_ctx*, K kernel, int threads, size_t smem) {
+    return occupancy_of((const void*)kernel, threads, smem);
+}
+
+static inline bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+// The LSD passes over `in` (n keys), writing through pp[0]/pp[1]; with PAIRS
+// the positions ping-pong through vpp and the last pass writes `vout`.
+template <typename U, int XF, bool PAIRS>
+static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0, uint32_t* vpp1, uint32_t* vout,
+                         size_t n, int write_keys_last, Plan** plan_out) {
+    using C = LsdCfg<U, PAIRS>;
+    constexpr int RADIX = C::RADIX, ND = C::ND, TILE = C::TILE;
+    const size_t tiles = (n + TILE - 1) / TILE;
+    const size_t max_portion_tiles = (size_t)(LB_VALUE / TILE);
+    const int portions = (int)((tiles + max_portion_tiles - 1) / max_portion_tiles);
+    const size_t portion_tiles = std::min(tiles, max_portion_tiles);
+    const int launches = ND * portions;
+    const MetaLayout m = MetaLayout::make(ND, RADIX, launches);
+    ts_status s;
+    if ((s = grow(c, c->meta, m.bytes, "sort metadata")) != TS_OK) return s;
+    const size_t lb_words = portion_tiles * RADIX;
+    if ((s = grow(c, c->lookback, 2 * lb_words * 4, "look-back")) != TS_OK) return s;
+    char* meta = (char*)c->meta.p;
+    ScanState* st = (ScanState*)(meta + m.scan_off);
+    Plan* plan = (Plan*)(meta + m.plan_off);
+    uint32_t* counters = (uint32_t*)(meta + m.counters_off);
+    unsigned long long* hist = (unsigned long long*)(meta + m.hist_off);
+    unsigned long long* bins = (unsigned long long*)(meta + m.bins_off);
+    unsigned long long* carry = (unsigned long long*)(meta + m.carry_off);
+    uint32_t* lb = (uint32_t*)c->lookback.p;
+    const int vec_ok = aligned16(in);
+
+    mark(c, "scan");
+    TS_CUDA(c, cudaMemsetAsync(meta, 0, m.zero_bytes(), c->stream));
+    TS_CUDA(c, cudaMemsetAsync(lb, 0, lb_words * 4, c->stream));
+    {
+        constexpr int T = 256;
+        const int grid = c->sm_count * 4;
+        k_scan<U, XF, T><<<grid, T, 0, c->stream>>>(in, n, C::BITS, ND, st, vec_ok);
+        ++c->launches;
+    }
+    mark(c, "histogram");
+    {
+        constexpr int T = 512;
+        const size_t smem = (size_t)ND * RADIX * (RADIX <= 256 ? 4 : 1) * 4;
+        auto kern = k_hist<U, XF, C::BITS, T>;
+        const int occ = occupancy(c, kern, T, smem);
+        kern<<<c->sm_count * occ, T, smem, c->stream>>>(in, n, st, hist, vec_ok);
+        ++c->launches;
+    }
+    mark(c, "plan");
+    k_plan<U, XF, C::BITS><<<1, 1024, 0, c->stream>>>(in, n, st, hist, bins, plan, PAIRS ? 1 : 0);
+    ++c->launches;
+    {
+        using Sm = SweepSmem<U, C::BITS, C::THREADS, C::IPT, PAIRS>;
+        auto kern = k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS>;
+        const int occ = occupancy(c, kern, C::THREADS, Sm::bytes);
+        SweepArgs<U, PAIRS> a{};
+        a.in = in;
+        a.pp[0] = pp0;
+        a.pp[1] = pp1;
+        a.vpp[0] = vpp0;
+        a.vpp[1] = vpp1;
+        a.vout = vout;
+        a.n = n;
+        a.write_keys_last = write_keys_last;
+        a.plan = plan;
+        a.bins = bins;
+        a.error = c->d_error;
+        int launch = 0;
+        for (int slot = 0; slot < ND; ++slot) {
+            for (int q = 0; q < portions; ++q, ++launch) {
+                a.slot = slot;
+                a.portion_begin = (size_t)q * portion_tiles * TILE;
+                a.portion_tiles = (int)std::min(portion_tiles, tiles - (size_t)q * portion_tiles);
+                a.carry_in = portions > 1 && q > 0 ? carry + (size_t)(q & 1) * RADIX : nullptr;
+                a.carry_out = portions > 1 ? carry + (size_t)((q + 1) & 1) * RADIX : nullptr;
+                a.lookback = lb + (size_t)(launch & 1) * lb_words;
+                a.lookback_next = lb + (size_t)((launch + 1) & 1) * lb_words;
+                a.lookback_words = lb_words;
+                a.tile_counter = counters + launch;
+                const int grid = (int)std::min((size_t)c->sm_count * occ, (size_t)a.portion_tiles);
+                mark(c, "onesweep");
+                kern<<<grid, C::THREADS, Sm::bytes, c->stream>>>(a);
+                ++c->launches;
+            }
+        }
+    }
+    *plan_out = plan;
+    return TS_OK;
+}
+
+template <typename U, int XF>
+ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
+    if (n <= 1) return TS_OK;
+    if constexpr (sizeof(U) == 1) {
+        if (n > (size_t)SMALL_MAX) {
+            ts_status s;
+            if ((s = grow(c, c->meta, 256 * 8, "counts")) != TS_OK) return s;
+            unsigned long long* h = (unsigned long long*)c->meta.p;
+            mark(c, "count8");
+            TS_CUDA(c, cudaMemsetAsync(h, 0, 256 * 8, c->stream));
+            k_count8<XF><<<c->sm_count * 4, 512, 0, c->stream>>>((const uint8_t*)d_data, n, h);
+        ++c->launches;
+            mark(c, "fill8");
+            const size_t work = (n + 15) / 16;
+            const int grid = (int)std::min((work + 255) / 256, (size_t)c->sm_count * 8);
+            k_fill8<XF><<<grid, 256, 0, c->stream>>>((uint8_t*)d_data, n, h);
+        ++c->launches;
+            mark(c, "end");
+            return TS_OK;
+        }
+    }
+    if (n <= (size_t)SMALL_MAX) {
+        mark(c, "small");
+        const int threads = (int)std::min<size_t>(SMALL_THREADS, std::max<size_t>(32, (n + 1) / 2));
+        k_small_sort<U, XF, false><<<1, threads, 0, c->stream>>>(d_data, d_data, nullptr, (int)n, 1);
+        ++c->launches;
+        mark(c, "end");
+        return TS_OK;
+    }
+    if constexpr (sizeof(U) > 1) {
+        ts_status s;
+        if (!d_alt) {
+            if ((s = grow(c, c->alt, n * sizeof(U), "scratch keys")) != TS_OK) return s;
+            d_alt = (U*)c->alt.p;
+        }
+        Plan* plan = nullptr;
+        if ((s = run_lsd<U, XF, false>(c, d_data, d_alt, d_data, nullptr, nullptr, nullptr, n, 1, &plan)) != TS_OK)
+            return s;
+        mark(c, "finish");
+        const int grid = c->sm_count * 4;
+        k_copy_back<U><<<grid, 512, 0, c->stream>>>(plan, d_alt, d_data, n, aligned16(d_alt) && aligned16(d_data));
+        ++c->launches;
+        k_reverse<U><<<grid, 512, 0, c->stream>>>(plan, d_data, n);
+        ++c->launches;
+        mark(c, "end");
+    }
+    return TS_OK;
+}
+
+template <typename U, int XF>
+ts_status order_device(ts_ctx* c, const U* d_keys, size_t n, uint32_t* d_order) {
+    if (n == 0) return TS_OK;
+    if (n > 0xffffffffull) return fail(c, TS_ERR_TOO_LARGE, "sort_by_key: more than u32::MAX elements");
+    if (n <= (size_t)SMALL_MAX) {
+        mark(c, "small");
+        const int threads = (int)std::min<size_t>(SMALL_THREADS, std::max<size_t>(32, (n + 1) / 2));
+        k_small_sort<U, XF, true><<<1, threads, 0, c->stream>>>(d_keys, nullptr, d_order, (int)n, 0);
+        ++c->launches;
+        mark(c, "end");
+        return TS_OK;
+    }
+    ts_status s;
+    if ((s = grow(c, c->alt, 2 * n * sizeof(U) + 16, "scratch keys")) != TS_OK) return s;
+    if ((s = grow(c, c->vals0, n * 4, "positions")) != TS_OK) return s;
+    if ((s = grow(c, c->vals1, n * 4, "positions")) != TS_OK) return s;
+    U* k0 = (U*)c->alt.p;
+    U* k1 = (U*)((char*)c->alt.p + (n * sizeof(U) + 15) / 16 * 16);
+    Plan* plan = nullptr;
+    if ((s = run_lsd<U, XF, true>(c, d_keys, k0, k1, (uint32_t*)c->vals0.p, (uint32_t*)c->vals1.p, d_order, n, 0,
+                                  &plan)) != TS_OK)
+        return s;
+    mark(c, "finish");
+    k_iota_if_unsorted<<<c->sm_count * 4, 512, 0, c->stream>>>(plan, d_order, n);
+        ++c->launches;
+    mark(c, "end");
+    return TS_OK;
+}
+
+}  // namespace ts
