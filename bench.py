@@ -228,8 +228,9 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def workload_config(name: str) -> dict:
-    kind, dist, lg = WORKLOADS[name]
+def workload_config(name: str, lg: int | None = None) -> dict:
+    kind, dist, lg0 = WORKLOADS[name]
+    lg = lg or lg0
     return {"workload": f"plain LSD sort of 2^{lg} {kind} keys, {DIST_NAMES[dist]} (seeded xorshift64), 8-bit digits",
             "name": name, "n": 1 << lg, "key_type": kind,
             "l2": "inputs larger than L2 (1 GiB vs 126 MB); each step sorts its own unsorted copy",
@@ -288,6 +289,7 @@ def main() -> None:
     ap.add_argument("--no-breakdown", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--log2n", type=int, default=None, help="override the workload's size (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -315,6 +317,8 @@ def main() -> None:
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
 
     kind, dist, lg = WORKLOADS[args.workload]
+    if args.log2n:
+        lg = args.log2n
     clocks = Clocks(local)
     clocks.start()
     r = bench_device(ts, torch, ctx, kind, dist, lg, args.steps, args.warmup, 0x9E3779B97F4A7C15 + rank, dist_mod,
@@ -339,13 +343,13 @@ def main() -> None:
     pass_bytes = n * w * 2
     achieved = pass_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None
     sort_bytes = n * w * (2 * live + 1)
-    traffic = ncu_traffic(f"onesweep_{kind}_2p{lg}.txt")
+    traffic = ncu_traffic(f"onesweep_{kind}_2p{lg}.md")
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GKeys/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": kind, "data": "synthetic (seeded xorshift64 keys)",
-        "config": workload_config(args.workload),
+        "config": workload_config(args.workload, lg),
         "bit_exact_checks": "sorted + sum/xor of the multiset" if r["ok"] else "FAILED",
         "roofline": {
             "bound": "hbm", "kernel": "k_onesweep (one live digit pass)",

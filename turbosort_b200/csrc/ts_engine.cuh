@@ -14,17 +14,25 @@
 
 #include "ts_ctx.h"
 #include "ts_lsd.cuh"
+#include "ts_onesweep.cuh"
 #include "ts_small.cuh"
 
 namespace ts {
 
-// Tile shapes per key width (threads x items per thread); 8-bit digits.
+// Tile shapes per key width; 8-bit digits. A tile is 16 warps x 32 lanes x
+// IPT keys.
 template <typename U, bool PAIRS>
 struct LsdCfg {
     static constexpr int BITS = 8;
     static constexpr int THREADS = 512;
-    static constexpr int IPT = sizeof(U) == 8 ? 8 : (PAIRS ? 12 : 16);
-    static constexpr int TILE = THREADS * IPT;
+    // sized so that two CTAs (double-buffered keys, staging tile, 32-bit
+    // per-warp counters) share one SM's shared memory
+    static constexpr int IPT = sizeof(U) == 8 ? 7 : (PAIRS ? 11 : (sizeof(U) == 4 ? 15 : 16));
+    static constexpr int NBUF = PAIRS ? 1 : 2;  // tiles of keys in flight per CTA
+    static constexpr int MATCH_MOD = 4;         // items with i % MATCH_MOD < MATCH_CNT use match.any
+    static constexpr int MATCH_CNT = 0;
+    using Smem = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
+    static constexpr int TILE = Smem::TILE;
     static constexpr int RADIX = 1 << BITS;
     static constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
 };
@@ -101,8 +109,8 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     }
     mark(c, "histogram");
     {
-        constexpr int T = 512;
-        const size_t smem = (size_t)ND * RADIX * (RADIX <= 256 ? 4 : 1) * 4;
+        constexpr int T = 1024;
+        const size_t smem = (size_t)ND * RADIX * hist_copies<RADIX, ND>() * 4;
         auto kern = k_hist<U, XF, C::BITS, T>;
         const int occ = occupancy(c, kern, T, smem);
         kern<<<c->sm_count * occ, T, smem, c->stream>>>(in, n, st, hist, vec_ok);
@@ -112,8 +120,10 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     k_plan<U, XF, C::BITS><<<1, 1024, 0, c->stream>>>(in, n, st, hist, bins, plan, PAIRS ? 1 : 0);
     ++c->launches;
     {
-        using Sm = SweepSmem<U, C::BITS, C::THREADS, C::IPT, PAIRS>;
-        auto kern = k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS>;
+        using Sm = typename C::Smem;
+        auto kern = n <= (size_t)0x7fffffff
+                        ? k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD, C::MATCH_CNT>
+                        : k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD, C::MATCH_CNT>;
         const int occ = occupancy(c, kern, C::THREADS, Sm::bytes);
         SweepArgs<U, PAIRS> a{};
         a.in = in;

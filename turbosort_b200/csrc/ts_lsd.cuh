@@ -19,6 +19,8 @@
 //               needed no pass
 #pragma once
 
+#include <type_traits>
+
 #include "ts_common.cuh"
 
 namespace ts {
@@ -116,19 +118,25 @@ __global__ void __launch_bounds__(THREADS) k_scan(const U* __restrict__ src, siz
 }
 
 // ---------------------------------------------------------------------------
-// k_hist: histograms of the varying digits in one read. Sub-histograms per
-// (lane % COPIES) keep lanes that share a digit off one address; the copy
-// index is the fastest-moving so those lanes also sit in different banks.
+// k_hist: histograms of the varying digits in one read. Each lane counts
+// into its own copy, and the copy index is the fastest-moving, so the 32
+// lanes of a warp always hit 32 different banks (no conflicts, no shared
+// addresses) whatever the digits are.
 // ---------------------------------------------------------------------------
+template <int RADIX, int ND>
+__host__ __device__ constexpr int hist_copies() {
+    return RADIX <= 256 ? (ND <= 4 ? 32 : 16) : 1;
+}
+
 template <typename U, int XF, int BITS, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
                                                   unsigned long long* __restrict__ ghist, int vec_ok) {
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
-    constexpr int COPIES = RADIX <= 256 ? 4 : 1;
+    constexpr int COPIES = hist_copies<RADIX, ND>();
     using V = Vec16<U>;
     constexpr int VN = V::N;
-    constexpr int UNROLL = 2;
+    constexpr int UNROLL = 4;
     extern __shared__ __align__(16) uint32_t h_s[];  // [ND][RADIX][COPIES]
     const unsigned long long diff = st->diff;
     uint32_t counted = 0;
@@ -137,42 +145,42 @@ __global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, siz
         if ((diff >> (d * BITS)) & (unsigned long long)(RADIX - 1)) counted |= 1u << d;
     for (int i = threadIdx.x; i < ND * RADIX * COPIES; i += THREADS) h_s[i] = 0;
     __syncthreads();
-    const int copy = threadIdx.x % COPIES;
-    const size_t per_iter = (size_t)THREADS * VN * UNROLL;
-    for (size_t it = (size_t)blockIdx.x * per_iter; it < n; it += (size_t)gridDim.x * per_iter) {
+    uint32_t* my_h = h_s + threadIdx.x % COPIES;
+    // one key into every counted digit's histogram; ALL: no digit is skipped
+    auto count = [&](U raw, auto all_tag) {
+        constexpr bool ALL = decltype(all_tag)::value;
+        const U key = to_key<U, XF>(raw);
 #pragma unroll
-        for (int u = 0; u < UNROLL; ++u) {
-            const size_t base = it + ((size_t)u * THREADS + threadIdx.x) * VN;
-            if (base >= n) break;
-            U k[VN];
-            int cnt = VN;
-            if (vec_ok && base + VN <= n) {
-                V x;
-                x.v = __ldcs(reinterpret_cast<const uint4*>(src + base));
+        for (int d = 0; d < ND; ++d)
+            if (ALL || (counted & (1u << d)))
+                atomicAdd(&my_h[(d * RADIX + digit_of(key, d * BITS, RADIX - 1)) * COPIES], 1u);
+    };
+    auto sweep = [&](auto all_tag) {
+        const size_t nvec = vec_ok ? n / VN : 0;
+        const size_t stride = (size_t)gridDim.x * THREADS;
+        const uint4* v4 = reinterpret_cast<const uint4*>(src);
+        for (size_t v0 = (size_t)blockIdx.x * THREADS + threadIdx.x; v0 < nvec; v0 += stride * UNROLL) {
+            V x[UNROLL];
 #pragma unroll
-                for (int e = 0; e < VN; ++e) k[e] = x.e[e];
-            } else {
-                cnt = (int)min((size_t)VN, n - base);
+            for (int u = 0; u < UNROLL; ++u)
+                if (v0 + u * stride < nvec) x[u].v = __ldcs(v4 + v0 + u * stride);
 #pragma unroll
-                for (int e = 0; e < VN; ++e) k[e] = e < cnt ? src[base + e] : (U)0;
-            }
+            for (int u = 0; u < UNROLL; ++u)
+                if (v0 + u * stride < nvec) {
 #pragma unroll
-            for (int e = 0; e < VN; ++e) {
-                if (e < cnt) {
-                    const U key = to_key<U, XF>(k[e]);
-#pragma unroll
-                    for (int d = 0; d < ND; ++d)
-                        if (counted & (1u << d))
-                            atomicAdd(&h_s[(d * RADIX + digit_of(key, d * BITS, RADIX - 1)) * COPIES + copy], 1u);
+                    for (int e = 0; e < VN; ++e) count(x[u].e[e], all_tag);
                 }
-            }
         }
-    }
+        for (size_t i = nvec * VN + (size_t)blockIdx.x * THREADS + threadIdx.x; i < n; i += stride)
+            count(src[i], all_tag);
+    };
+    if (counted == (1u << ND) - 1) sweep(std::true_type{});
+    else sweep(std::false_type{});
     __syncthreads();
     for (int i = threadIdx.x; i < ND * RADIX; i += THREADS) {
         uint32_t s = 0;
 #pragma unroll
-        for (int c = 0; c < COPIES; ++c) s += h_s[i * COPIES + c];
+        for (int c = 0; c < COPIES; ++c) s += h_s[i * COPIES + ((c + i) & (COPIES - 1))];
         if (s) atomicAdd(&ghist[i], (unsigned long long)s);
     }
 }
@@ -230,262 +238,6 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
     }
 }
 
-// ---------------------------------------------------------------------------
-// k_onesweep: one live digit pass. Persistent CTAs take tiles in order from a
-// counter, so a tile only ever waits on tiles already taken by running CTAs.
-// ---------------------------------------------------------------------------
-template <typename U, bool PAIRS>
-struct SweepArgs {
-    const U* in;                 // slot 0 source
-    U* pp[2];                    // ping-pong: slot j writes pp[j & 1], reads pp[(j - 1) & 1]
-    const uint32_t* vin;         // unused: slot 0 starts from positions 0..n-1
-    uint32_t* vpp[2];            // position ping-pong (PAIRS)
-    uint32_t* vout;              // last slot's positions: the order (PAIRS)
-    size_t n;                    // keys in the whole sort
-    size_t portion_begin;        // first key of this launch's portion
-    int portion_tiles;           // tiles in this portion
-    int slot;                    // which live pass this launch is
-    int write_keys_last;         // PAIRS: does the last pass write keys too
-    const Plan* plan;
-    const unsigned long long* bins;   // [ND][RADIX] exclusive scans
-    const unsigned long long* carry_in;  // [RADIX] keys of this digit in earlier portions, or null
-    unsigned long long* carry_out;       // written by the portion's last tile, or null
-    uint32_t* lookback;          // [portion_tiles][RADIX], zero when the launch starts
-    uint32_t* lookback_next;     // the next launch's region: this launch zeroes it
-    size_t lookback_words;       // words per region (a multiple of 4)
-    uint32_t* tile_counter;      // zeroed before the launch
-    uint32_t* error;
-};
-
-template <typename U, int BITS, int THREADS, int IPT, bool PAIRS>
-struct SweepSmem {
-    static constexpr int RADIX = 1 << BITS;
-    static constexpr int TILE = THREADS * IPT;
-    static constexpr int WARPS = THREADS / 32;
-    using CT = typename std::conditional<(RADIX > 256), uint16_t, uint32_t>::type;
-    static constexpr size_t keys_off = 0;
-    static constexpr size_t vals_off = (keys_off + sizeof(U) * TILE + 15) / 16 * 16;
-    static constexpr size_t cnt_off = (vals_off + (PAIRS ? 4 * TILE : 0) + 15) / 16 * 16;
-    static constexpr size_t gbase_off = (cnt_off + sizeof(CT) * WARPS * RADIX + 15) / 16 * 16;
-    static constexpr size_t misc_off = gbase_off + 8 * RADIX;
-    static constexpr size_t bytes = misc_off + 4 * 64;
-};
-
-template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS>
-__global__ void __launch_bounds__(THREADS, 2) k_onesweep(SweepArgs<U, PAIRS> a) {
-    using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS>;
-    using CT = typename L::CT;
-    constexpr int RADIX = L::RADIX;
-    constexpr int TILE = L::TILE;
-    constexpr int WARPS = L::WARPS;
-    constexpr uint32_t MASK = RADIX - 1;
-    constexpr int DPT = RADIX >= THREADS ? RADIX / THREADS : 1;   // digits per owner thread
-    constexpr int OWNERS = RADIX / DPT;
-    static_assert(TILE < 65536 || RADIX <= 256, "16-bit counters need tiles below 65536 keys");
-    static_assert(RADIX % DPT == 0 && OWNERS <= THREADS, "digit ownership");
-
-    const int mode = a.plan->mode, n_live = a.plan->n_live;
-    if (mode != MODE_SORT || a.slot >= n_live) return;
-    const int pass = a.plan->pass[a.slot];
-    const int shift = pass * BITS;
-    const bool first = a.slot == 0;
-    const bool last = a.slot == n_live - 1;
-    const U* __restrict__ src = first ? a.in : a.pp[(a.slot - 1) & 1];
-    U* __restrict__ dst = a.pp[a.slot & 1];
-    const uint32_t* __restrict__ vsrc = first ? nullptr : a.vpp[(a.slot - 1) & 1];
-    uint32_t* __restrict__ vdst = last ? a.vout : a.vpp[a.slot & 1];
-    const bool write_keys = !PAIRS || !last || a.write_keys_last;
-    const unsigned long long* __restrict__ bins = a.bins + (size_t)pass * RADIX;
-
-    extern __shared__ __align__(16) unsigned char smem[];
-    U* keys_s = reinterpret_cast<U*>(smem + L::keys_off);
-    uint32_t* vals_s = reinterpret_cast<uint32_t*>(smem + L::vals_off);
-    CT* cnt_s = reinterpret_cast<CT*>(smem + L::cnt_off);
-    long long* gbase_s = reinterpret_cast<long long*>(smem + L::gbase_off);
-    int* misc_s = reinterpret_cast<int*>(smem + L::misc_off);  // [0] tile, [32..] warp totals
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const size_t portion_end = min(a.n, a.portion_begin + (size_t)a.portion_tiles * TILE);
-
-    // The previous launch used the other region; clear it for the next one.
-    {
-        uint4* z = reinterpret_cast<uint4*>(a.lookback_next);
-        const size_t nz = a.lookback_words / 4;
-        for (size_t i = (size_t)blockIdx.x * THREADS + tid; i < nz; i += (size_t)gridDim.x * THREADS)
-            z[i] = make_uint4(0u, 0u, 0u, 0u);
-    }
-
-    for (;;) {
-        if (tid == 0) misc_s[0] = (int)atomicAdd(a.tile_counter, 1u);
-        __syncthreads();
-        const int t = misc_s[0];
-        if (t >= a.portion_tiles) break;
-        const size_t tile_base = a.portion_begin + (size_t)t * TILE;
-        const int tile_n = (int)min((size_t)TILE, portion_end - tile_base);
-
-        for (int i = tid; i < WARPS * RADIX; i += THREADS) cnt_s[i] = 0;
-
-        // ---- load: warp-striped, item i of lane l is tile index w*32*IPT + i*32 + l
-        U k[IPT];
-        uint32_t v[IPT];
-        const int wbase = warp * 32 * IPT + lane;
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const int idx = wbase + i * 32;
-            if (idx < tile_n) {
-                k[i] = __ldcs(src + tile_base + idx);
-                if constexpr (PAIRS) v[i] = first ? (uint32_t)(tile_base + idx) : __ldcs(vsrc + tile_base + idx);
-            } else {
-                k[i] = 0;
-                if constexpr (PAIRS) v[i] = 0;
-            }
-        }
-        if (first) {
-#pragma unroll
-            for (int i = 0; i < IPT; ++i) k[i] = to_key<U, XF>(k[i]);
-        }
-        __syncthreads();
-
-        // ---- rank inside the warp: stable, one match.any per item
-        CT* my_cnt = cnt_s + warp * RADIX;
-        uint32_t rank[IPT];
-        const uint32_t lt = lanemask_lt();
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const bool valid = wbase + i * 32 < tile_n;
-            const uint32_t d = valid ? digit_of(k[i], shift, MASK) : (uint32_t)RADIX;
-            const uint32_t peers = __match_any_sync(0xffffffffu, d);
-            const uint32_t leader = 31 - __clz(peers);
-            uint32_t c = 0;
-            if (valid) c = my_cnt[d];
-            __syncwarp();
-            if (valid && lane == (int)leader) my_cnt[d] = (CT)(c + __popc(peers));
-            __syncwarp();
-            rank[i] = c + __popc(peers & lt);
-        }
-        __syncthreads();
-
-        // ---- per digit: prefix over warps, tile count, publish, tile-local start
-        uint32_t tcount[DPT];
-        if (tid < OWNERS) {
-#pragma unroll
-            for (int q = 0; q < DPT; ++q) {
-                const int r = tid * DPT + q;
-                uint32_t s = 0;
-#pragma unroll 4
-                for (int w = 0; w < WARPS; ++w) {
-                    const uint32_t c = cnt_s[w * RADIX + r];
-                    cnt_s[w * RADIX + r] = (CT)s;
-                    s += c;
-                }
-                tcount[q] = s;
-                st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, (t == 0 ? LB_FLAG_INC : LB_FLAG_AGG) | s);
-            }
-        }
-        // block exclusive scan of the tile counts over digits (owners only hold data)
-        uint32_t own = 0;
-        if (tid < OWNERS) {
-#pragma unroll
-            for (int q = 0; q < DPT; ++q) own += tcount[q];
-        }
-        uint32_t x = own;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) misc_s[32 + warp] = (int)x;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t wt = lane < WARPS ? (uint32_t)misc_s[32 + lane] : 0u;
-            uint32_t z = wt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
-                if (lane >= o) z += y;
-            }
-            if (lane < WARPS) misc_s[32 + lane] = (int)(z - wt);
-        }
-        __syncthreads();
-        uint32_t lstart[DPT];
-        if (tid < OWNERS) {
-            uint32_t run = (uint32_t)misc_s[32 + warp] + x - own;
-#pragma unroll
-            for (int q = 0; q < DPT; ++q) {
-                lstart[q] = run;
-                run += tcount[q];
-                const int r = tid * DPT + q;
-#pragma unroll 4
-                for (int w = 0; w < WARPS; ++w) cnt_s[w * RADIX + r] = (CT)(cnt_s[w * RADIX + r] + lstart[q]);
-            }
-        }
-        __syncthreads();
-
-        // ---- reorder the tile in shared memory by digit
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            if (wbase + i * 32 < tile_n) {
-                const uint32_t d = digit_of(k[i], shift, MASK);
-                const uint32_t pos = (uint32_t)my_cnt[d] + rank[i];
-                if (pos < (uint32_t)TILE) {
-                    keys_s[pos] = k[i];
-                    if constexpr (PAIRS) vals_s[pos] = v[i];
-                } else {
-                    atomicOr(a.error, ERR_BOUNDS);
-                }
-            }
-        }
-
-        // ---- decoupled look-back: keys of each digit in earlier tiles
-        if (tid < OWNERS) {
-#pragma unroll
-            for (int q = 0; q < DPT; ++q) {
-                const int r = tid * DPT + q;
-                uint32_t excl = 0;
-                if (t > 0) {
-                    int j = t - 1;
-                    uint32_t spins = 0;
-                    while (j >= 0) {
-                        const uint32_t w = ld_relaxed_gpu(a.lookback + (size_t)j * RADIX + r);
-                        const uint32_t f = w & ~LB_VALUE;
-                        if (f == 0) {
-                            if (++spins > SPIN_LIMIT) {
-                                atomicOr(a.error, ERR_TIMEOUT);
-                                break;
-                            }
-                            continue;
-                        }
-                        excl += w & LB_VALUE;
-                        if (f == LB_FLAG_INC) break;
-                        --j;
-                    }
-                    st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, LB_FLAG_INC | (excl + tcount[q]));
-                }
-                const unsigned long long carry = a.carry_in ? a.carry_in[r] : 0ull;
-                gbase_s[r] = (long long)(bins[r] + carry + excl) - (long long)lstart[q];
-                if (a.carry_out && t == a.portion_tiles - 1) a.carry_out[r] = carry + excl + tcount[q];
-            }
-        }
-        __syncthreads();
-
-        // ---- write runs per digit: consecutive threads, consecutive addresses
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const int s = i * THREADS + tid;
-            if (s < tile_n) {
-                const U key = keys_s[s];
-                const uint32_t d = digit_of(key, shift, MASK);
-                const unsigned long long pos = (unsigned long long)(gbase_s[d] + s);
-                if (pos < a.n) {
-                    if (write_keys) dst[pos] = last ? from_key<U, XF>(key) : key;
-                    if constexpr (PAIRS) vdst[pos] = vals_s[s];
-                } else {
-                    atomicOr(a.error, ERR_BOUNDS);
-                }
-            }
-        }
-    }
-}
 
 // ---------------------------------------------------------------------------
 // Finishing kernels, each a no-op unless the plan calls for it.

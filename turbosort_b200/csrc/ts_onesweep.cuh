@@ -1,0 +1,398 @@
+// ts_onesweep.cuh — one stable LSD scatter pass (src/radix/scatter.rs:26-247)
+// per launch, as a decoupled-look-back "onesweep" over tiles of keys.
+//
+// Per tile (THREADS x IPT keys), in a persistent CTA that takes tiles in
+// order from a counter:
+//   1. the keys arrive in shared memory by one bulk copy (cp.async.bulk, no
+//      multicast), issued one tile ahead so the next tile streams in while
+//      this one is ranked;
+//   2. a counting pass builds per-warp digit counts, the tile's
+//      digit counts are published to the look-back array at once, and the
+//      tile-local start of every (digit, warp) run is scanned;
+//   3. a ranking pass finds each key's equals inside its warp with one ballot
+//      per digit bit and writes the key straight to its sorted place in a
+//      shared staging tile (stable: warp order, then item order, then lane);
+//   4. the digit owners finish the look-back (keys of their digit in all
+//      earlier tiles) while no other work waits on it;
+//   5. the staged tile goes out as runs per digit: consecutive threads write
+//      consecutive addresses.
+// The key transform (src/key.rs:135-197) is applied as the first pass reads
+// and undone as the last pass writes. With PAIRS a u32 position travels with
+// each key (the stable order() of src/by_key.rs:254-310); the first pass
+// makes the positions itself.
+#pragma once
+
+#include <type_traits>
+
+#include "ts_common.cuh"
+
+namespace ts {
+
+template <typename U, bool PAIRS>
+struct SweepArgs {
+    const U* in;                 // slot 0 source
+    U* pp[2];                    // ping-pong: slot j writes pp[j & 1], reads pp[(j - 1) & 1]
+    uint32_t* vpp[2];            // position ping-pong (PAIRS)
+    uint32_t* vout;              // last slot's positions: the order (PAIRS)
+    size_t n;                    // keys in the whole sort
+    size_t portion_begin;        // first key of this launch's portion
+    int portion_tiles;           // tiles in this portion
+    int slot;                    // which live pass this launch is
+    int write_keys_last;         // PAIRS: does the last pass write keys too
+    const Plan* plan;
+    const unsigned long long* bins;      // [ND][RADIX] exclusive scans
+    const unsigned long long* carry_in;  // [RADIX] keys of this digit in earlier portions, or null
+    unsigned long long* carry_out;       // written by the portion's last tile, or null
+    uint32_t* lookback;          // [portion_tiles][RADIX], zero when the launch starts
+    uint32_t* lookback_next;     // the next launch's region: this launch zeroes it
+    size_t lookback_words;       // words per region (a multiple of 4)
+    uint32_t* tile_counter;      // zeroed before the launch
+    uint32_t* error;
+};
+
+template <typename U, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF>
+struct SweepSmem {
+    static constexpr int RADIX = 1 << BITS;
+    static constexpr int WARPS = THREADS / 32;
+    static constexpr int RANK_WARPS = WARPS;
+    static constexpr int TILE = RANK_WARPS * 32 * IPT;
+    static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t kbuf_off = 0;                                             // [NBUF][TILE] U
+    static constexpr size_t vbuf_off = al(kbuf_off + (size_t)NBUF * TILE * sizeof(U));  // [NBUF][TILE] u32
+    static constexpr size_t sk_off = al(vbuf_off + (PAIRS ? (size_t)NBUF * TILE * 4 : 0));  // [TILE] U sorted
+    static constexpr size_t sv_off = al(sk_off + (size_t)TILE * sizeof(U));           // [TILE] u32 sorted
+    static constexpr size_t cnt_off = al(sv_off + (PAIRS ? (size_t)TILE * 4 : 0));    // [RANK_WARPS][RADIX] u32
+    static constexpr size_t gbase_off = al(cnt_off + (size_t)RANK_WARPS * RADIX * 4);  // [RADIX] i64
+    static constexpr size_t bar_off = al(gbase_off + (size_t)RADIX * 8);              // [2] mbarrier
+    static constexpr size_t misc_off = bar_off + 16;                                  // ints
+    static constexpr size_t bytes = misc_off + 4 * 64;
+    static_assert(TILE * sizeof(U) % 16 == 0, "bulk copies move multiples of 16 bytes");
+};
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// The lanes of a warp whose BITS-bit digit equals this lane's. One ballot per
+// digit bit gives the warp's bit-planes; lane L then builds the entry of two
+// small tables for the digit values it stands for (its low 5 bits, and its
+// low 3 bits for the top digit bits), and each lane reads the two entries of
+// its own digit with a shuffle. xl[b] / xh[b] hold, per lane, all ones where
+// the lane's index has bit b clear (set up once by peer_masks_init).
+template <int BITS>
+struct PeerMasks {
+    static_assert(BITS >= 1 && BITS <= 10, "two lookup tables cover digits of up to 10 bits");
+    static constexpr int LO = BITS < 5 ? BITS : 5;
+    static constexpr int HI = BITS - LO;
+    uint32_t xl[LO];
+    uint32_t xh[HI > 0 ? HI : 1];
+    __device__ __forceinline__ void init(int lane) {
+#pragma unroll
+        for (int b = 0; b < LO; ++b) xl[b] = ((lane >> b) & 1) ? 0u : 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < HI; ++b) xh[b] = ((lane >> b) & 1) ? 0u : 0xffffffffu;
+    }
+    __device__ __forceinline__ uint32_t peers(uint32_t d) const {
+        uint32_t lo = 0xffffffffu, hi = 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < LO; ++b) lo &= __ballot_sync(0xffffffffu, (d >> b) & 1u) ^ xl[b];
+#pragma unroll
+        for (int b = 0; b < HI; ++b) hi &= __ballot_sync(0xffffffffu, (d >> (LO + b)) & 1u) ^ xh[b];
+        uint32_t p = __shfl_sync(0xffffffffu, lo, (int)(d & ((1u << LO) - 1)));
+        if constexpr (HI > 0) p &= __shfl_sync(0xffffffffu, hi, (int)(d >> LO));
+        return p;
+    }
+};
+
+__device__ __forceinline__ void ld_relaxed_gpu_v4(const uint32_t* p, uint32_t (&v)[4]) {
+    asm volatile("ld.relaxed.gpu.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+                 : "l"(p)
+                 : "memory");
+}
+__device__ __forceinline__ void st_relaxed_gpu_v4(uint32_t* p, const uint32_t (&v)[4]) {
+    asm volatile("st.relaxed.gpu.global.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(v[0]), "r"(v[1]), "r"(v[2]),
+                 "r"(v[3])
+                 : "memory");
+}
+
+// Items i with i % MATCH_MOD < MATCH_CNT find their equal digits with the
+// match.any instruction, which runs on a different pipe from the ballots; the
+// rest use PeerMasks. The split keeps both pipes busy.
+template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
+          int MATCH_CNT>
+__global__ void __launch_bounds__(THREADS, 2) k_onesweep(SweepArgs<U, PAIRS> a) {
+    using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
+    using OFF = typename std::conditional<BIG, long long, int>::type;
+    constexpr int RADIX = L::RADIX;
+    constexpr int TILE = L::TILE;
+    constexpr int RANK_WARPS = L::RANK_WARPS;
+    constexpr uint32_t MASK = RADIX - 1;
+    constexpr int OWNERS = RADIX < THREADS ? RADIX : THREADS;  // threads that own digits
+    constexpr int DPT = RADIX / OWNERS;                          // digits per owner thread
+    constexpr int OWNER_WARPS = (OWNERS + 31) / 32;
+    constexpr int SCATTER_IT = (TILE + THREADS - 1) / THREADS;
+    static_assert(RADIX % OWNERS == 0 && OWNER_WARPS <= RANK_WARPS, "digit ownership");
+
+    const int mode = a.plan->mode, n_live = a.plan->n_live;
+    if (mode != MODE_SORT || a.slot >= n_live) return;
+    const int pass = a.plan->pass[a.slot];
+    const int shift = pass * BITS;
+    const bool first = a.slot == 0;
+    const bool last = a.slot == n_live - 1;
+    const U* __restrict__ src = first ? a.in : a.pp[(a.slot - 1) & 1];
+    U* __restrict__ dst = a.pp[a.slot & 1];
+    const uint32_t* __restrict__ vsrc = (PAIRS && !first) ? a.vpp[(a.slot - 1) & 1] : nullptr;
+    uint32_t* __restrict__ vdst = last ? a.vout : a.vpp[a.slot & 1];
+    const bool write_keys = !PAIRS || !last || a.write_keys_last;
+    const unsigned long long* __restrict__ bins = a.bins + (size_t)pass * RADIX;
+
+    extern __shared__ __align__(128) unsigned char smem[];
+    U* kbuf = reinterpret_cast<U*>(smem + L::kbuf_off);
+    uint32_t* vbuf = reinterpret_cast<uint32_t*>(smem + L::vbuf_off);
+    U* sk = reinterpret_cast<U*>(smem + L::sk_off);
+    uint32_t* sv = reinterpret_cast<uint32_t*>(smem + L::sv_off);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(smem + L::cnt_off);
+    OFF* gbase = reinterpret_cast<OFF*>(smem + L::gbase_off);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::bar_off);
+    int* misc = reinterpret_cast<int*>(smem + L::misc_off);  // [0..2] tile ids, [32..] warp totals
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt = lanemask_lt();
+    PeerMasks<BITS> pm;
+    pm.init(lane);
+    const size_t portion_end = min(a.n, a.portion_begin + (size_t)a.portion_tiles * TILE);
+    const bool bulk_ok = ((uintptr_t)src & 15) == 0 && (!PAIRS || first || ((uintptr_t)vsrc & 15) == 0);
+
+    // The previous launch used the other look-back region; clear it for the next.
+    {
+        uint4* z = reinterpret_cast<uint4*>(a.lookback_next);
+        const size_t nz = a.lookback_words / 4;
+        for (size_t i = (size_t)blockIdx.x * THREADS + tid; i < nz; i += (size_t)gridDim.x * THREADS)
+            z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    for (int i = tid; i < RANK_WARPS * RADIX; i += THREADS) cnt[i] = 0;
+    if (tid == 0) {
+        for (int b = 0; b < NBUF; ++b) mbar_init(&bars[b], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    // thread 0: start the copy of tile t into buffer b (full tiles from an
+    // aligned source; anything else arrives without data and is loaded below)
+    auto issue = [&](int t, int b) {
+        const size_t base = a.portion_begin + (size_t)t * TILE;
+        const bool full = base + TILE <= portion_end;
+        if (full && bulk_ok) {
+            fence_proxy_async_smem();
+            const uint32_t bytes = TILE * sizeof(U) + ((PAIRS && !first) ? TILE * 4 : 0);
+            mbar_arrive_expect_tx(&bars[b], bytes);
+            bulk_g2s(kbuf + (size_t)b * TILE, src + base, TILE * sizeof(U), &bars[b]);
+            if constexpr (PAIRS) {
+                if (!first) bulk_g2s(vbuf + (size_t)b * TILE, vsrc + base, TILE * 4, &bars[b]);
+            }
+        } else {
+            mbar_arrive_expect_tx(&bars[b], 0);
+        }
+    };
+
+    uint32_t parity = 0;  // bit b: the phase buffer b's barrier completes next
+
+    // One tile. FULL (a compile-time tag) drops every per-key bounds test:
+    // only the last tile of a portion can be partial.
+    auto process = [&](int t, int b, auto full_tag) {
+        constexpr bool FULL = decltype(full_tag)::value;
+        const size_t tile_base = a.portion_begin + (size_t)t * TILE;
+        const int tile_n = FULL ? TILE : (int)min((size_t)TILE, portion_end - tile_base);
+        U* kb = kbuf + (size_t)b * TILE;
+        uint32_t* vb = vbuf + (size_t)b * TILE;
+
+        // ---- 1. the tile's keys in shared memory
+        if (!mbar_wait(&bars[b], (parity >> b) & 1u)) atomicOr(a.error, ERR_TIMEOUT);
+        parity ^= 1u << b;
+        if (!(FULL && bulk_ok)) {
+            for (int i = tid; i < tile_n; i += THREADS) {
+                kb[i] = src[tile_base + i];
+                if constexpr (PAIRS) {
+                    if (!first) vb[i] = vsrc[tile_base + i];
+                }
+            }
+            __syncthreads();
+        }
+
+        // ---- 2. per-warp digit counts
+        const int wbase = warp * 32 * IPT + lane;
+        uint32_t* my_cnt = cnt + warp * RADIX;
+        {
+#pragma unroll
+            for (int i = 0; i < IPT; ++i) {
+                if (FULL || wbase + i * 32 < tile_n) {
+                    U k = kb[wbase + i * 32];
+                    if (first) k = to_key<U, XF>(k);
+                    atomicAdd(&my_cnt[digit_of(k, shift, MASK)], 1u);
+                }
+            }
+        }
+        __syncthreads();
+
+        // digit owners: prefix over warps, publish the tile's counts, tile-local starts
+        uint32_t tcount[DPT];
+        uint32_t own = 0;
+        if (tid < OWNERS) {
+#pragma unroll
+            for (int q = 0; q < DPT; ++q) {
+                const int r = tid * DPT + q;
+                uint32_t s = 0;
+#pragma unroll
+                for (int w = 0; w < RANK_WARPS; ++w) {
+                    const uint32_t c = cnt[w * RADIX + r];
+                    cnt[w * RADIX + r] = s;
+                    s += c;
+                }
+                tcount[q] = s;
+                own += s;
+                st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, (t == 0 ? LB_FLAG_INC : LB_FLAG_AGG) | s);
+            }
+        }
+        uint32_t x = own;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31 && warp < OWNER_WARPS) misc[32 + warp] = (int)x;
+        __syncthreads();
+        uint32_t lstart[DPT];
+        if (tid < OWNERS) {
+            uint32_t run = x - own;
+            for (int w = 0; w < warp; ++w) run += (uint32_t)misc[32 + w];
+#pragma unroll
+            for (int q = 0; q < DPT; ++q) {
+                const int r = tid * DPT + q;
+                lstart[q] = run;
+#pragma unroll
+                for (int w = 0; w < RANK_WARPS; ++w) cnt[w * RADIX + r] += run;
+                run += tcount[q];
+            }
+        }
+        __syncthreads();
+
+        {
+            // ---- 3. rank among equal digits in the warp and stage in sorted order
+#pragma unroll
+            for (int i = 0; i < IPT; ++i) {
+                const int idx = wbase + i * 32;
+                const bool valid = FULL || idx < tile_n;
+                U k = kb[FULL ? idx : min(idx, TILE - 1)];
+                if (first) k = to_key<U, XF>(k);
+                const uint32_t d = digit_of(k, shift, MASK);
+                uint32_t peers;
+                if ((i % MATCH_MOD) < MATCH_CNT) peers = __match_any_sync(0xffffffffu, d);
+                else peers = pm.peers(d);
+                if (!FULL) peers &= __ballot_sync(0xffffffffu, valid);
+                if (valid) {
+                    const uint32_t c = my_cnt[d];
+                    my_cnt[d] = c + __popc(peers);
+                    const uint32_t pos = c + __popc(peers & lt);
+                    sk[pos] = k;
+                    if constexpr (PAIRS) sv[pos] = first ? (uint32_t)(tile_base + idx) : vb[idx];
+                }
+                __syncwarp();
+            }
+        }
+
+        // ---- 4. owners: keys of their digit in earlier tiles (the decoupled
+        // look-back; predecessors have had the whole ranking pass to publish),
+        // then the digit's global base
+        if (tid < OWNERS) {
+#pragma unroll
+            for (int q = 0; q < DPT; ++q) {
+                const int r = tid * DPT + q;
+                uint32_t excl = 0;
+                if (t > 0) {
+                    int j = t - 1;
+                    uint32_t spins = 0;
+                    while (j >= 0) {
+                        const uint32_t w = ld_relaxed_gpu(a.lookback + (size_t)j * RADIX + r);
+                        const uint32_t f = w & ~LB_VALUE;
+                        if (f == 0) {
+                            if (++spins > SPIN_LIMIT) {
+                                atomicOr(a.error, ERR_TIMEOUT);
+                                break;
+                            }
+                            continue;
+                        }
+                        excl += w & LB_VALUE;
+                        if (f == LB_FLAG_INC) break;
+                        --j;
+                    }
+                    st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, LB_FLAG_INC | (excl + tcount[q]));
+                }
+                const unsigned long long carry = a.carry_in ? a.carry_in[r] : 0ull;
+                unsigned long long start = bins[r] + carry + excl;
+                if (start + tcount[q] > a.n) {  // only after a timeout: keep every write in bounds
+                    atomicOr(a.error, ERR_BOUNDS);
+                    start = a.n - tcount[q];
+                }
+                gbase[r] = (OFF)((long long)start - (long long)lstart[q]);
+                if (a.carry_out && t == a.portion_tiles - 1) a.carry_out[r] = carry + excl + tcount[q];
+            }
+        }
+        __syncthreads();
+
+        // ---- 5. runs per digit to global memory
+#pragma unroll
+        for (int i = 0; i < SCATTER_IT; ++i) {
+            const int s = i * THREADS + tid;
+            if ((TILE % THREADS == 0 || i < SCATTER_IT - 1 || s < TILE) && (FULL || s < tile_n)) {
+                const U k = sk[s];
+                const OFF p = gbase[digit_of(k, shift, MASK)] + (OFF)s;
+                if (write_keys) dst[p] = last ? from_key<U, XF>(k) : k;
+                if constexpr (PAIRS) vdst[p] = sv[s];
+            }
+        }
+        // clear the counters for the next tile (no one reads them past step 3)
+        for (int i = tid; i < RANK_WARPS * RADIX; i += THREADS) cnt[i] = 0;
+    };
+    auto run_tile = [&](int t, int b) {
+        if (a.portion_begin + (size_t)(t + 1) * TILE <= portion_end) process(t, b, std::true_type{});
+        else process(t, b, std::false_type{});
+    };
+
+    if constexpr (NBUF == 2) {
+        if (tid == 0) {
+            const int t0 = (int)atomicAdd(a.tile_counter, 1u);
+            misc[0] = t0;
+            if (t0 < a.portion_tiles) issue(t0, 0);
+        }
+        __syncthreads();
+        int cur = misc[0], b = 0, it = 0;
+        while (cur < a.portion_tiles) {
+            if (tid == 0) {  // take the next tile and start its copy into the other buffer
+                const int nx = (int)atomicAdd(a.tile_counter, 1u);
+                misc[1 + (it & 1)] = nx;
+                if (nx < a.portion_tiles) issue(nx, b ^ 1);
+            }
+            run_tile(cur, b);
+            cur = misc[1 + (it & 1)];
+            b ^= 1;
+            ++it;
+            __syncthreads();
+        }
+    } else {
+        for (;;) {
+            if (tid == 0) {
+                const int t = (int)atomicAdd(a.tile_counter, 1u);
+                misc[0] = t;
+                if (t < a.portion_tiles) issue(t, 0);
+            }
+            __syncthreads();
+            const int t = misc[0];
+            if (t >= a.portion_tiles) break;
+            run_tile(t, 0);
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace ts
