@@ -1,0 +1,36 @@
+"""The C++ API (include/turbosort.hpp) on the crate's README examples and
+larger slices: compiled with g++ against libturbosort_b200.so and run."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "turbosort_b200")
+
+
+def _build(tmp_path):
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    exe = str(tmp_path / "api_example")
+    cmd = [cxx, "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp",
+           "api_example.cpp"), "-L", LIBDIR, "-lturbosort_b200", f"-Wl,-rpath,{LIBDIR}", "-o", exe]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_cpp_api_compiles(tmp_path):
+    import turbosort_b200  # noqa: F401  (the library must exist)
+
+    assert os.path.exists(turbosort_b200.LIB_PATH)
+    _build(tmp_path)
+
+
+@pytest.mark.gpu
+def test_cpp_api_examples(tmp_path):
+    exe = _build(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "ok"
