@@ -107,6 +107,23 @@ ts_status ts_apply_order(ts_ctx *ctx, void *data, size_t n, size_t elem_size, co
 ts_status ts_apply_order_dev(ts_ctx *ctx, void *d_data, size_t n, size_t elem_size, const uint32_t *d_order,
                              size_t order_len);
 
+/* No counterpart in the reference. The device sort of u32 keys for callers
+ * that cannot allocate device memory: those whose framework owns all device
+ * memory and forbids raw cudaMalloc, those on latency-critical paths where an
+ * allocation's implicit synchronisation would stall other streams, and those
+ * held to a memory budget fixed at start-up. It needs no context and calls no
+ * allocating routine: its scratch is one fixed device array inside the library
+ * (about 18 MB, held by every GPU that loads the library until exit), so it
+ * sorts at most TS_NOALLOC_MAX_KEYS keys and returns TS_ERR_TOO_LARGE above
+ * that. The sort runs on `stream` (a cudaStream_t, or NULL for the legacy
+ * default stream) and the call returns when it is done. The first call on a
+ * device looks up the array's address there; make that first call before any
+ * stream capture. Calls share the array: calls that overlap on the GPU race,
+ * so one process runs one at a time and callers in several processes or on
+ * several streams must serialise them. */
+#define TS_NOALLOC_MAX_KEYS ((size_t)1 << 22)
+ts_status ts_sort_dev_noalloc_u32(uint32_t *d_data, size_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
