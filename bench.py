@@ -279,6 +279,71 @@ def bench_device(ts, torch, ctx, kind, dist, lg, steps, warmup, seed, dist_mod, 
     return {"ms_total": ms, "launches": launches, "timings": tm, "ok": ok, "live": live, "n": n, "w": w}
 
 
+def bench_by_key(ts, torch, ctx, lg, steps, warmup, peak):
+    """Config 3: stable sort_by_key_with_buffer of 2^lg records keyed by u64
+    Zipf(1.1) keys over 2^20 distinct values; the records are 16 bytes
+    {u64 id = original index, u32 a, u32 b}; then apply_order on a second
+    u32 slice. A step = order() + moving both slices, all on the device."""
+    from turbosort_b200 import workloads as W
+
+    n = 1 << lg
+    keys = W.zipf_u64(n)
+    dev = f"cuda:{ctx.device}"
+    dk = torch.from_numpy(keys.view(np.int64)).to(dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    rec = torch.empty((n, 4), dtype=torch.int32, device=dev)
+    ids = torch.arange(n, dtype=torch.int64, device=dev)
+    rec[:, 0:2] = ids.view(torch.int32).view(n, 2)
+    rec[:, 2:4] = torch.randint(-2**31, 2**31 - 1, (n, 2), dtype=torch.int32, device=dev, generator=g)
+    side = torch.randint(-2**31, 2**31 - 1, (n,), dtype=torch.int32, device=dev, generator=g)
+    side0 = side.clone()
+    order = torch.empty(n, dtype=torch.int32, device=dev)
+    lib = ts.lib()
+
+    def step():
+        ctx._check(lib.ts_sort_keys_order_dev_u64(ctx.handle, dk.data_ptr(), n, order.data_ptr()))
+        ctx._check(lib.ts_apply_order_dev(ctx.handle, rec.data_ptr(), n, 16, order.data_ptr(), n))
+        ctx._check(lib.ts_apply_order_dev(ctx.handle, side.data_ptr(), n, 4, order.data_ptr(), n))
+
+    step()  # checked below: records and side slice moved once
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    o = order.to(torch.int64)
+    kk = dk[o].cpu().numpy().view(np.uint64)
+    oo = o.cpu().numpy()
+    sorted_ok = bool(np.all(kk[1:] >= kk[:-1]))
+    eq = kk[1:] == kk[:-1]
+    stable_ok = bool(np.all(oo[1:][eq] > oo[:-1][eq]))
+    perm_ok = bool(np.array_equal(np.sort(oo), np.arange(n)))
+    rec_ok = bool(torch.equal(rec[:, 0:2].contiguous().view(torch.int64).view(-1), o))
+    side_ok = bool(torch.equal(side, side0[o]))
+    ok = sorted_ok and stable_ok and perm_ok and rec_ok and side_ok
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.reset_timings()
+    ctx.enable_timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ctx.enable_timing(False)
+    tm = ctx.timings()
+    ms = e0.elapsed_time(e1) / steps
+    sweep_ms = tm.get("onesweep", (0.0, 0))[0] / steps
+    gather_ms = tm.get("gather", (0.0, 0))[0] / steps
+    del rec, side, side0, dk, order
+    torch.cuda.empty_cache()
+    return {"gkeys_s": round(n / (ms / 1e3) / 1e9, 3), "ms": round(ms, 3), "order_ms": round(ms - gather_ms, 3),
+            "apply_order_ms": round(gather_ms, 3), "onesweep_ms": round(sweep_ms, 3),
+            "what": "order() of 2^27 Zipf u64 keys + apply_order of 16-byte records and a u32 slice",
+            "ok": ok, "checks": "sorted, stable (equal keys keep input order), permutation, records and side slice moved"}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,6 +481,7 @@ def main() -> None:
                         "sort_frac": round(sb / (st / 1e3) / 1e9 / peak, 3),
                         "pass_frac": round(rr["n"] * rr["w"] * 2 / (ow / 1e3) / 1e9 / peak, 3) if ow else None,
                         "ok": rr["ok"]}
+        bd["c3_by_key_zipf_u64_2p27"] = bench_by_key(ts, torch, ctx, 27, max(3, args.steps // 2), 3, peak)
         line["breakdown"] = bd
 
     if rank == 0:

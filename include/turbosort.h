@@ -107,6 +107,41 @@ ts_status ts_apply_order(ts_ctx *ctx, void *data, size_t n, size_t elem_size, co
 ts_status ts_apply_order_dev(ts_ctx *ctx, void *d_data, size_t n, size_t elem_size, const uint32_t *d_order,
                              size_t order_len);
 
+/* Segmented batch sort (no single counterpart in the crate: the crate sorts
+ * each slice with its own `sort` call, src/lib.rs:99, as its small_batches
+ * benchmark does, benches/sort_bench.rs:229-250). Sorts every segment
+ * data[offsets[i] .. offsets[i+1]) in place, independently, for i < n_seg;
+ * offsets holds n_seg + 1 non-decreasing entries ending within n. One device
+ * launch sorts the whole batch: segments are binned by length (32 keys and
+ * fewer: a warp each; up to 16384 (8192 for 8-byte keys): on chip; longer: a CTA each through L2;
+ * host calls send segments above 2^22 keys to the device-wide sort). The _dev
+ * form replays a captured CUDA graph when called again with the same
+ * pointers and sizes. Segments must hold fewer than 2^31 keys. */
+#define TS_DECLARE_SEGMENTS(SUF, T)                                                                       \
+    ts_status ts_sort_segments_##SUF(ts_ctx *ctx, T *data, size_t n, const uint64_t *offsets, size_t n_seg); \
+    ts_status ts_sort_segments_dev_##SUF(ts_ctx *ctx, T *d_data, size_t n, const uint64_t *d_offsets, size_t n_seg);
+
+TS_DECLARE_SEGMENTS(u8, uint8_t)
+TS_DECLARE_SEGMENTS(u16, uint16_t)
+TS_DECLARE_SEGMENTS(u32, uint32_t)
+TS_DECLARE_SEGMENTS(u64, uint64_t)
+TS_DECLARE_SEGMENTS(i8, int8_t)
+TS_DECLARE_SEGMENTS(i16, int16_t)
+TS_DECLARE_SEGMENTS(i32, int32_t)
+TS_DECLARE_SEGMENTS(i64, int64_t)
+TS_DECLARE_SEGMENTS(f32, float)
+TS_DECLARE_SEGMENTS(f64, double)
+
+/* The on-chip method of each segment length bin (32,256] (256,1024]
+ * (1024,4096] (4096,16384 or 8192], per key width: 0 bitonic network, 1 radix with
+ * 4-bit digits, 2 radix with 8-bit digits. ts_segments_autotune times every
+ * method on synthetic batches of each bin on this GPU and keeps the fastest;
+ * ts_segments_methods reads (set = 0) or sets (set = 1) the four methods. */
+ts_status ts_segments_autotune(ts_ctx *ctx, size_t key_bytes);
+ts_status ts_segments_methods(ts_ctx *ctx, size_t key_bytes, int *methods, int set);
+/* Capture and replay CUDA graphs for repeated segmented sorts (on by default). */
+ts_status ts_ctx_use_graphs(ts_ctx *ctx, int on);
+
 /* No counterpart in the reference. The device sort of u32 keys for callers
  * that cannot allocate device memory: those whose framework owns all device
  * memory and forbids raw cudaMalloc, those on latency-critical paths where an

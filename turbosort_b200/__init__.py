@@ -24,7 +24,8 @@ import numpy as np
 
 __all__ = [
     "Context", "SortByKeyBuffer", "TurbosortError", "apply_order", "default_context", "lib", "sort",
-    "sort_by_key", "sort_by_key_with_buffer", "sort_parallel", "sort_with_buffer", "TYPES",
+    "sort_by_key", "sort_by_key_with_buffer", "sort_parallel", "sort_segments", "sort_with_buffer", "segments_autotune",
+    "segments_methods", "TYPES",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -105,6 +106,19 @@ def lib() -> ctypes.CDLL:
                     f = getattr(L, name + t)
                     f.argtypes = args
                     f.restype = st
+            for t in TYPES:
+                getattr(L, f"ts_sort_segments_{t}").argtypes = [vp, vp, sz, vp, sz]
+                getattr(L, f"ts_sort_segments_{t}").restype = st
+                getattr(L, f"ts_sort_segments_dev_{t}").argtypes = [vp, vp, sz, vp, sz]
+                getattr(L, f"ts_sort_segments_dev_{t}").restype = st
+            L.ts_segments_autotune.argtypes = [vp, sz]
+            L.ts_segments_autotune.restype = st
+            L.ts_segments_methods.argtypes = [vp, sz, vp, i]
+            L.ts_segments_methods.restype = st
+            L.ts_ctx_use_graphs.argtypes = [vp, i]
+            L.ts_ctx_use_graphs.restype = st
+            L.ts_ctx_launches.argtypes = [vp]
+            L.ts_ctx_launches.restype = ctypes.c_ulonglong
             L.ts_apply_order.argtypes = [vp, vp, sz, sz, vp, sz]
             L.ts_apply_order.restype = st
             L.ts_apply_order_dev.argtypes = [vp, vp, sz, sz, vp, sz]
@@ -285,6 +299,40 @@ def apply_order(data, order, ctx: Context | None = None) -> None:
     elem = data.itemsize * (int(np.prod(data.shape[1:])) if data.ndim > 1 else 1)
     o = np.ascontiguousarray(order, dtype=np.uint32)
     ctx._check(lib().ts_apply_order(ctx.handle, _host_ptr(data), n, elem, o.ctypes.data, o.size))
+
+
+def sort_segments(data, offsets, ctx: Context | None = None) -> None:
+    """Sort every segment data[offsets[i]:offsets[i+1]] in place, independently
+    (the crate's sort applied to each slice), in one device launch. `offsets`
+    holds n_seg + 1 non-decreasing entries (numpy uint64 for host data, a CUDA
+    int64 tensor for device data)."""
+    ctx = ctx or default_context(data.device.index if _is_torch(data) else 0)
+    t = _type_of(data)
+    if _dev(data):
+        n_seg = offsets.numel() - 1
+        ctx._check(getattr(lib(), f"ts_sort_segments_dev_{t}")(ctx.handle, data.data_ptr(), data.numel(),
+                                                                offsets.data_ptr(), max(n_seg, 0)))
+        return
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    ctx._check(getattr(lib(), f"ts_sort_segments_{t}")(ctx.handle, _host_ptr(data), data.size, o.ctypes.data,
+                                                        max(o.size - 1, 0)))
+
+
+def segments_methods(key_bytes: int, ctx: Context | None = None, methods=None) -> list[int]:
+    """Read (or set) the on-chip method of each segment length bin for keys of
+    `key_bytes`: 0 bitonic, 1 radix with 4-bit digits, 2 radix with 8-bit digits."""
+    ctx = ctx or default_context(0)
+    arr = (ctypes.c_int * 4)(*(methods or [0, 0, 0, 0]))
+    ctx._check(lib().ts_segments_methods(ctx.handle, key_bytes, arr, 1 if methods is not None else 0))
+    return list(arr)
+
+
+def segments_autotune(key_bytes: int, ctx: Context | None = None) -> list[int]:
+    """Time each method on synthetic batches of every length bin on this GPU
+    and keep the fastest; returns the chosen methods."""
+    ctx = ctx or default_context(0)
+    ctx._check(lib().ts_segments_autotune(ctx.handle, key_bytes))
+    return segments_methods(key_bytes, ctx)
 
 
 def _key_array(items, key, dtype):

@@ -59,7 +59,7 @@ int occupancy_of(const void* kernel, int threads, size_t smem) {
 }
 
 void mark(ts_ctx* c, const char* name) {
-    if (!c->timing) return;
+    if (!c->timing || c->capturing) return;
     cudaEvent_t ev;
     if (!c->spare_events.empty()) {
         ev = c->spare_events.back();
@@ -89,7 +89,7 @@ void fold_marks(ts_ctx* c) {
 }
 
 // Wait for the stream, then report what the kernels flagged.
-static ts_status finish(ts_ctx* c) {
+ts_status finish(ts_ctx* c) {
     uint32_t host_err = 0;
     cudaError_t e = cudaMemcpyAsync(&host_err, c->d_error, 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_error, 0, 4, c->stream);
@@ -230,8 +230,9 @@ void ts_ctx_destroy(ts_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather})
+    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg})
         if (b->p) cudaFree(b->p);
+    if (c->seg_graph) cudaGraphExecDestroy(c->seg_graph);
     if (c->d_error) cudaFree(c->d_error);
     for (auto& m : c->marks) cudaEventDestroy(m.second);
     for (auto ev : c->spare_events) cudaEventDestroy(ev);

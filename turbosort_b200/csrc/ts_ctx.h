@@ -35,7 +35,16 @@ struct ts_ctx {
     ts::DevBuf meta;               // scan state, plan, histograms, scans, counters, carries
     ts::DevBuf lookback;           // two look-back regions
     ts::DevBuf gather;             // apply_order staging
+    ts::DevBuf seg;                // segmented sort: plan, work counter, bin lists, offsets
     uint32_t* d_error = nullptr;   // kernel-reported errors, read and cleared by the host
+
+    // segmented sort: the method of each on-chip length bin per key width
+    // (1, 2, 4, 8 bytes), set by the autotuner; and the last captured graph
+    int seg_methods[4][4] = {{0, 2, 2, 2}, {0, 2, 2, 2}, {0, 2, 2, 2}, {0, 2, 2, 2}};
+    bool use_graphs = true;
+    bool capturing = false;
+    cudaGraphExec_t seg_graph = nullptr;
+    size_t seg_graph_key[10] = {};
 
     std::string last_error;
     unsigned long long launches = 0;   // kernels this context has launched
@@ -55,6 +64,8 @@ void mark(ts_ctx* c, const char* name);
 void fold_marks(ts_ctx* c);
 
 ts_status fail(ts_ctx* c, ts_status s, const std::string& msg);
+// Wait for the context's stream and report what the kernels flagged.
+ts_status finish(ts_ctx* c);
 ts_status cuda_fail(ts_ctx* c, cudaError_t e, const char* where);
 ts_status grow(ts_ctx* c, DevBuf& b, size_t bytes, const char* what);
 

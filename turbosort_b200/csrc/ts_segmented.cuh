@@ -1,0 +1,401 @@
+// ts_segmented.cuh — many independent slices sorted in one persistent launch.
+//
+// The crate sorts each slice with its own call (the pattern of its
+// small_batches benchmark, benches/sort_bench.rs:229-250, and of
+// compare/src/main.rs:49-51); here a batch of slices given by offsets is
+// sorted at once. k_seg_bin puts each segment in a length bin; k_seg_sort is
+// one persistent launch whose CTAs take work items largest first:
+//   LARGE  one segment above the shared-memory capacity: a CTA-level LSD over
+//          its varying digits, tile by tile through a global scratch copy
+//          (the segment stays in L2), with running per-digit offsets;
+//   BLOCK  one segment of up to CAP keys, sorted entirely on chip: keys in
+//          registers, one shared staging buffer, one stable pass per varying
+//          digit (radix with 4- or 8-bit digits) or a bitonic network, as the
+//          tuned configuration of its length bin says;
+//   WARP   up to 32 segments of at most 32 keys, one per warp, bitonic in
+//          registers with shuffles.
+// Every result equals the crate's sort of that slice (src/dispatch.rs:31):
+// the sorted order of radix keys is unique.
+#pragma once
+
+#include <type_traits>
+
+#include "ts_common.cuh"
+#include "ts_onesweep.cuh"
+
+namespace ts {
+
+constexpr int SEG_THREADS = 1024;
+constexpr int SEG_WARPS = SEG_THREADS / 32;
+constexpr int SEG_BLOCK_BINS = 4;  // BLOCK length bins: (32,256] (256,1024] (1024,4096] (4096,CAP]
+constexpr int SEG_BIN_WARP = SEG_BLOCK_BINS;
+constexpr int SEG_BIN_LARGE = SEG_BLOCK_BINS + 1;
+constexpr int SEG_NBINS = SEG_BLOCK_BINS + 2;
+
+enum SegMethod : int { SEG_BITONIC = 0, SEG_RADIX4 = 1, SEG_RADIX8 = 2 };
+
+template <typename U>
+struct SegCfg {
+    static constexpr int IPT = sizeof(U) == 8 ? 8 : 16;  // keys per thread held in registers
+    static constexpr int CAP = SEG_THREADS * IPT;        // largest segment sorted on chip
+    static constexpr int LARGE_IPT = sizeof(U) == 8 ? 8 : 16;
+    static constexpr int LARGE_TILE = SEG_THREADS * LARGE_IPT;
+};
+
+struct SegPlan {
+    unsigned int count[SEG_NBINS];  // segments per bin
+    unsigned int items;             // work items in total
+    int method[SEG_BLOCK_BINS];     // tuned method per BLOCK bin
+    unsigned int pad[6];
+};
+
+__host__ __device__ inline int seg_bin_of(unsigned long long len, int cap) {
+    if (len <= 32) return SEG_BIN_WARP;
+    if (len > (unsigned long long)cap) return SEG_BIN_LARGE;
+    if (len <= 256) return 0;
+    if (len <= 1024) return 1;
+    if (len <= 4096) return 2;
+    return 3;
+}
+
+// Work items, largest first: LARGE segments, BLOCK bins from the longest
+// down, then groups of SEG_WARPS tiny segments.
+__device__ __forceinline__ void seg_item(const SegPlan& p, unsigned int item, int* bin, unsigned int* first) {
+    unsigned int base = 0;
+    if (item < base + p.count[SEG_BIN_LARGE]) {
+        *bin = SEG_BIN_LARGE;
+        *first = item - base;
+        return;
+    }
+    base += p.count[SEG_BIN_LARGE];
+    for (int b = SEG_BLOCK_BINS - 1; b >= 0; --b) {
+        if (item < base + p.count[b]) {
+            *bin = b;
+            *first = item - base;
+            return;
+        }
+        base += p.count[b];
+    }
+    *bin = SEG_BIN_WARP;
+    *first = (item - base) * SEG_WARPS;
+}
+
+static __global__ void k_seg_items(SegPlan* plan) {
+    if (threadIdx.x == 0) {
+        unsigned int t = plan->count[SEG_BIN_LARGE] + (plan->count[SEG_BIN_WARP] + SEG_WARPS - 1) / SEG_WARPS;
+        for (int b = 0; b < SEG_BLOCK_BINS; ++b) t += plan->count[b];
+        plan->items = t;
+    }
+}
+
+// ---- WARP: bitonic network over 32 lanes ---------------------------------
+template <typename U, int XF>
+__device__ __forceinline__ void seg_warp_sort(U* seg, int len, int lane) {
+    U v = lane < len ? to_key<U, XF>(seg[lane]) : (U)~(U)0;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const U o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+            v = keep_min ? (o < v ? o : v) : (o > v ? o : v);
+        }
+    }
+    if (lane < len) seg[lane] = from_key<U, XF>(v);
+}
+
+// ---- BLOCK: on-chip sorts ---------------------------------------------------
+// Bitonic over the next power of two in shared memory.
+template <typename U, int XF>
+__device__ void seg_block_bitonic(U* seg, int len, U* sm) {
+    int p2 = 1;
+    while (p2 < len) p2 <<= 1;
+    for (int i = threadIdx.x; i < p2; i += SEG_THREADS) sm[i] = i < len ? to_key<U, XF>(seg[i]) : (U)~(U)0;
+    __syncthreads();
+    for (int k = 2; k <= p2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < p2 / 2; i += SEG_THREADS) {
+                // the i-th compare-exchange pair of this step
+                const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+                const int hi = lo | j;
+                const bool up = (lo & k) == 0;
+                const U a = sm[lo], b = sm[hi];
+                if ((a > b) == up) {
+                    sm[lo] = b;
+                    sm[hi] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < len; i += SEG_THREADS) seg[i] = from_key<U, XF>(sm[i]);
+}
+
+// One stable pass of the on-chip LSD: keys in registers (warp-striped: item i
+// of lane l of warp w is key w*32*IPT + i*32 + l), written to their sorted
+// places in `sm`. cnt is [SEG_WARPS][RADIX].
+template <typename U, int BITS, int IPT>
+__device__ __forceinline__ void seg_rank_pass(const U (&k)[IPT], int wbase, int ipt, int len, int shift, U* sm,
+                                              uint32_t* cnt, int* warp_tot, const PeerMasks<BITS>& pm,
+                                              uint32_t* lstart_out = nullptr, uint32_t* count_out = nullptr) {
+    constexpr int RADIX = 1 << BITS;
+    constexpr uint32_t MASK = RADIX - 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint32_t* my_cnt = cnt + warp * RADIX;
+    for (int i = tid; i < SEG_WARPS * RADIX; i += SEG_THREADS) cnt[i] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < IPT; ++i)
+        if (i < ipt && wbase + i * 32 < len) atomicAdd(&my_cnt[digit_of(k[i], shift, MASK)], 1u);
+    __syncthreads();
+    // per digit: prefix over warps; then an exclusive scan over digits
+    uint32_t own = 0;
+    for (int r = tid; r < RADIX; r += SEG_THREADS) {
+        uint32_t s = 0;
+        for (int w = 0; w < SEG_WARPS; ++w) {
+            const uint32_t c = cnt[w * RADIX + r];
+            cnt[w * RADIX + r] = s;
+            s += c;
+        }
+        own = s;  // RADIX <= SEG_THREADS: one digit per thread
+    }
+    uint32_t x = own;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = (int)x;
+    __syncthreads();
+    if (tid < RADIX) {
+        uint32_t run = x - own;
+        for (int w = 0; w < warp; ++w) run += (uint32_t)warp_tot[w];
+        for (int w = 0; w < SEG_WARPS; ++w) cnt[w * RADIX + tid] += run;
+        if (lstart_out) {
+            lstart_out[tid] = run;
+            count_out[tid] = own;
+        }
+    }
+    __syncthreads();
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        if (i >= ipt) break;  // uniform: ipt is the same for the whole block
+        const bool valid = wbase + i * 32 < len;
+        const uint32_t d = digit_of(k[i], shift, MASK);
+        const uint32_t peers = pm.peers(d) & __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const uint32_t c = my_cnt[d];
+            my_cnt[d] = c + __popc(peers);
+            sm[c + __popc(peers & lt)] = k[i];
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
+template <typename U, int XF, int BITS>
+__device__ void seg_block_radix(U* seg, int len, U* sm, uint32_t* cnt, int* warp_tot, unsigned long long* red) {
+    constexpr int IPT = SegCfg<U>::IPT;
+    constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // spread the keys over the warps: each warp takes a contiguous run
+    const int ipt = (len + SEG_THREADS - 1) / SEG_THREADS;  // items per lane actually used
+    const int wbase = warp * 32 * ipt + lane;
+    PeerMasks<BITS> pm;
+    pm.init(lane);
+    U k[IPT];
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const int idx = wbase + i * 32;
+        k[i] = (i < ipt && idx < len) ? to_key<U, XF>(seg[idx]) : (U)0;
+    }
+    if (threadIdx.x == 0) *red = 0;
+    __syncthreads();
+    // the bits in which some key differs from the first: only those digits get a pass
+    const U first = to_key<U, XF>(seg[0]);
+    unsigned long long d = 0;
+#pragma unroll
+    for (int i = 0; i < IPT; ++i)
+        if (i < ipt && wbase + i * 32 < len) d |= (unsigned long long)(k[i] ^ first);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d |= __shfl_xor_sync(0xffffffffu, d, o);
+    if (lane == 0) atomicOr(red, d);
+    __syncthreads();
+    const unsigned long long vary = *red;
+    for (int p = 0; p < ND; ++p) {
+        if (((vary >> (p * BITS)) & ((1ull << BITS) - 1)) == 0) continue;
+        seg_rank_pass<U, BITS, IPT>(k, wbase, ipt, len, p * BITS, sm, cnt, warp_tot, pm);
+        // reload in the same warp-striped layout for the next pass
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int idx = wbase + i * 32;
+            k[i] = (i < ipt && idx < len) ? sm[idx] : (U)0;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const int idx = wbase + i * 32;
+        if (i < ipt && idx < len) seg[idx] = from_key<U, XF>(k[i]);
+    }
+}
+
+// ---- LARGE: a CTA-level LSD through the segment's scratch copy ------------
+struct SegSmem {
+    // offsets of the shared-memory areas (bytes) for key type U
+    template <typename U>
+    static constexpr size_t sm_bytes() { return (size_t)SegCfg<U>::CAP * sizeof(U); }
+    template <typename U>
+    static constexpr size_t cnt_off() { return sm_bytes<U>(); }
+    template <typename U>
+    static constexpr size_t hist_off() { return cnt_off<U>() + (size_t)SEG_WARPS * 256 * 4; }
+    template <typename U>
+    static constexpr size_t run_off() { return hist_off<U>() + (size_t)8 * 256 * 4; }
+    template <typename U>
+    static constexpr size_t misc_off() { return run_off<U>() + (size_t)3 * 256 * 4; }
+    template <typename U>
+    static constexpr size_t bytes() { return misc_off<U>() + 512; }
+};
+
+template <typename U, int XF>
+__device__ void seg_large_sort(U* seg, U* alt, int len, U* sm, uint32_t* cnt, int* warp_tot, unsigned long long* red,
+                               uint32_t* hist, uint32_t* run, uint32_t* lst, uint32_t* tcnt) {
+    constexpr int RADIX = 256;
+    constexpr int ND = (int)sizeof(U);
+    constexpr int IPT = SegCfg<U>::LARGE_IPT;
+    constexpr int TILE = SegCfg<U>::LARGE_TILE;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    PeerMasks<8> pm;
+    pm.init(lane);
+    // 1. one read: the bits that vary and the histogram of every digit
+    for (int i = tid; i < ND * RADIX; i += SEG_THREADS) hist[i] = 0;
+    if (tid == 0) *red = 0;
+    __syncthreads();
+    const U first = to_key<U, XF>(seg[0]);
+    unsigned long long d = 0;
+    for (int i = tid; i < len; i += SEG_THREADS) {
+        const U k = to_key<U, XF>(seg[i]);
+        d |= (unsigned long long)(k ^ first);
+#pragma unroll
+        for (int p = 0; p < ND; ++p) atomicAdd(&hist[p * RADIX + digit_of(k, p * 8, RADIX - 1)], 1u);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d |= __shfl_xor_sync(0xffffffffu, d, o);
+    if (lane == 0) atomicOr(red, d);
+    __syncthreads();
+    const unsigned long long vary = *red;
+    int last_p = -1;
+    for (int p = 0; p < ND; ++p)
+        if ((vary >> (p * 8)) & 0xff) last_p = p;
+    // 2. one pass per varying digit, tile by tile, with running digit offsets
+    bool in_alt = false, first_pass = true;
+    for (int p = 0; p < ND; ++p) {
+        if (((vary >> (p * 8)) & 0xff) == 0) continue;
+        const U* src = in_alt ? alt : seg;
+        U* dst = in_alt ? seg : alt;
+        const bool last = p == last_p;
+        // exclusive scan of this digit's histogram into run[]
+        {
+            const uint32_t own = tid < RADIX ? hist[p * RADIX + tid] : 0u;
+            uint32_t x = own;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) warp_tot[warp] = (int)x;
+            __syncthreads();
+            if (tid < RADIX) {
+                uint32_t r = x - own;
+                for (int w = 0; w < warp; ++w) r += (uint32_t)warp_tot[w];
+                run[tid] = r;
+            }
+            __syncthreads();
+        }
+        for (int t0 = 0; t0 < len; t0 += TILE) {
+            const int tn = min(TILE, len - t0);
+            const int ipt = (tn + SEG_THREADS - 1) / SEG_THREADS;
+            const int wbase = warp * 32 * ipt + lane;
+            U k[IPT];
+#pragma unroll
+            for (int i = 0; i < IPT; ++i) {
+                const int idx = wbase + i * 32;
+                U v = (i < ipt && idx < tn) ? src[t0 + idx] : (U)0;
+                k[i] = first_pass ? to_key<U, XF>(v) : v;
+            }
+            seg_rank_pass<U, 8, IPT>(k, wbase, ipt, tn, p * 8, sm, cnt, warp_tot, pm, lst, tcnt);
+            for (int s2 = tid; s2 < tn; s2 += SEG_THREADS) {
+                const U key = sm[s2];
+                const uint32_t dg = digit_of(key, p * 8, RADIX - 1);
+                dst[run[dg] + (uint32_t)s2 - lst[dg]] = last ? from_key<U, XF>(key) : key;
+            }
+            __syncthreads();
+            if (tid < RADIX) run[tid] += tcnt[tid];
+            __syncthreads();
+        }
+        in_alt = !in_alt;
+        first_pass = false;
+    }
+    if (in_alt) {
+        for (int i = tid; i < len; i += SEG_THREADS) seg[i] = alt[i];
+    }
+}
+
+// ---- the persistent launch ---------------------------------------------------
+struct SegMethods {
+    int m[SEG_BLOCK_BINS];
+};
+
+template <typename U, int XF>
+__global__ void __launch_bounds__(SEG_THREADS, 1)
+    k_seg_sort(U* __restrict__ data, U* __restrict__ alt, const unsigned long long* __restrict__ offsets,
+               const unsigned int* __restrict__ lists, size_t n_seg, const SegPlan* __restrict__ plan,
+               unsigned int* __restrict__ counter, SegMethods methods) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    U* sm = reinterpret_cast<U*>(smem);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(smem + SegSmem::cnt_off<U>());
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + SegSmem::hist_off<U>());
+    uint32_t* run = reinterpret_cast<uint32_t*>(smem + SegSmem::run_off<U>());
+    uint32_t* lst = run + 256;
+    uint32_t* tcnt = run + 512;
+    int* misc = reinterpret_cast<int*>(smem + SegSmem::misc_off<U>());
+    int* warp_tot = misc;                                            // [32]
+    unsigned long long* red = reinterpret_cast<unsigned long long*>(misc + 32);
+    int* item_s = misc + 40;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned int items = plan->items;
+    for (;;) {
+        if (threadIdx.x == 0) *item_s = (int)atomicAdd(counter, 1u);
+        __syncthreads();
+        const unsigned int item = (unsigned int)*item_s;
+        __syncthreads();
+        if (item >= items) break;
+        int bin;
+        unsigned int first;
+        seg_item(*plan, item, &bin, &first);
+        if (bin == SEG_BIN_WARP) {
+            const unsigned int idx = first + warp;
+            if (idx < plan->count[SEG_BIN_WARP]) {
+                const unsigned int s = lists[(size_t)SEG_BIN_WARP * n_seg + idx];
+                const unsigned long long b = offsets[s];
+                seg_warp_sort<U, XF>(data + b, (int)(offsets[s + 1] - b), lane);
+            }
+        } else {
+            const unsigned int s = lists[(size_t)bin * n_seg + first];
+            const unsigned long long b = offsets[s];
+            const int len = (int)(offsets[s + 1] - b);
+            if (bin == SEG_BIN_LARGE) {
+                seg_large_sort<U, XF>(data + b, alt + b, len, sm, cnt, warp_tot, red, hist, run, lst, tcnt);
+            } else {
+                const int m = methods.m[bin];
+                if (m == SEG_BITONIC) seg_block_bitonic<U, XF>(data + b, len, sm);
+                else if (m == SEG_RADIX4) seg_block_radix<U, XF, 4>(data + b, len, sm, cnt, warp_tot, red);
+                else seg_block_radix<U, XF, 8>(data + b, len, sm, cnt, warp_tot, red);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace ts
