@@ -344,6 +344,80 @@ def bench_by_key(ts, torch, ctx, lg, steps, warmup, peak):
             "ok": ok, "checks": "sorted, stable (equal keys keep input order), permutation, records and side slice moved"}
 
 
+def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True):
+    """Config 4: 100,000 segments with lengths log-uniform on [1, 65536], keys
+    of random bits, sorted in one segmented launch (graph replay, autotuned
+    on-chip methods), against one plain sort call per segment."""
+    from turbosort_b200 import workloads as W
+
+    lengths = W.segment_lengths(100_000)
+    offs = np.zeros(lengths.size + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum(lengths)
+    n = int(offs[-1])
+    bits = W.plain_u32(n, seed=0x2545F4914F6CDD1D)
+    host = bits.view(np.float32) if kind == "f32" else bits
+    dev = f"cuda:{ctx.device}"
+    methods = ts.segments_autotune(4, ctx)
+    master = torch.from_numpy(bits.view(np.int32)).to(dev)
+    d = torch.empty_like(master)
+    d_off = torch.from_numpy(offs.view(np.int64)).to(dev)
+    tdt = torch.float32 if kind == "f32" else torch.uint32
+    for _ in range(warmup):
+        d.copy_(master)
+        ts.sort_segments(d.view(tdt), d_off, ctx)
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(steps):
+        d.copy_(master)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ts.sort_segments(d.view(tdt), d_off, ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    ms = tot / steps
+    out = d.cpu().numpy().view(host.dtype)
+    k = radix_keys_np(out)
+    inside = np.ones(n - 1, dtype=bool)
+    inside[(offs[1:-1] - 1).astype(np.int64)] = False  # pairs that straddle a boundary
+    ok = bool(np.all(k[1:][inside] >= k[:-1][inside]))
+    ok &= checksums(out) == checksums(host)
+    rng = np.random.default_rng(1)
+    for s in rng.integers(0, lengths.size, size=50):
+        lo, hi = int(offs[s]), int(offs[s + 1])
+        ok &= bool(np.array_equal(np.sort(radix_keys_np(host[lo:hi])), k[lo:hi]))
+    res = {"gkeys_s": round(n / (ms / 1e3) / 1e9, 3), "ms": round(ms, 3), "keys": n, "segments": int(lengths.size),
+           "methods_per_bin": methods, "ok": ok,
+           "roofline_frac": round(2 * n * 4 / (ms / 1e3) / 1e9 / measured_peak_gbs()[0], 3)}
+    if per_segment:
+        # the crate's way: one sort call per slice (here the plain device sort per segment)
+        lib = ts.lib()
+        f = getattr(lib, f"ts_sort_dev_{kind}")
+        base = d.data_ptr()
+        d.copy_(master)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        h = ctx.handle
+        for s in range(lengths.size):
+            lo = int(offs[s])
+            f(h, base + 4 * lo, int(lengths[s]))
+        e1.record()
+        torch.cuda.synchronize()
+        ps_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+        out2 = d.cpu().numpy().view(host.dtype)
+        res["per_segment_ms"] = round(ps_ms, 1)
+        res["speedup_vs_per_segment"] = round(ps_ms / ms, 1)
+        res["ok"] = res["ok"] and out2.tobytes() == out.tobytes()
+    del master, d, d_off
+    torch.cuda.empty_cache()
+    return res
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -482,6 +556,8 @@ def main() -> None:
                         "pass_frac": round(rr["n"] * rr["w"] * 2 / (ow / 1e3) / 1e9 / peak, 3) if ow else None,
                         "ok": rr["ok"]}
         bd["c3_by_key_zipf_u64_2p27"] = bench_by_key(ts, torch, ctx, 27, max(3, args.steps // 2), 3, peak)
+        for kind in ("u32", "f32"):
+            bd[f"c4_segments_{kind}"] = bench_segments(ts, torch, ctx, kind, max(3, args.steps // 2), 2)
         line["breakdown"] = bd
 
     if rank == 0:
