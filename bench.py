@@ -418,6 +418,72 @@ def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True):
     return res
 
 
+def bench_learned(ts, torch, ctx, kind, steps, warmup, peak, lg=28):
+    """Config 5: the learned-partition sort against the plain device LSD on the
+    same 2^lg keys: f64 lognormal(0, 2), u64 from 8 Gaussians (means in
+    [0, 2^60], sigma 2^40), f32 uniform [0, 1) with 10% duplicates. Model: 1024
+    leaves, 1% sample, 2^14 buckets, fallback at 4x the mean bucket. Both
+    outputs must be identical bit for bit."""
+    from turbosort_b200 import workloads as W
+
+    n = 1 << lg
+    host = {"lognormal_f64": W.lognormal_f64, "gauss_mix_u64": W.gauss_mix_u64,
+            "unit_f32_dups": W.unit_f32_dups}[kind](n)
+    w = host.itemsize
+    dev = f"cuda:{ctx.device}"
+    tdt = {"lognormal_f64": torch.float64, "gauss_mix_u64": torch.uint64, "unit_f32_dups": torch.float32}[kind]
+    ibits = torch.int64 if w == 8 else torch.int32
+    master = torch.from_numpy(host.view(np.int64 if w == 8 else np.int32)).to(dev)
+    del host
+    d = torch.empty_like(master)
+    p = ts.learned_params()
+
+    def timed(fn):
+        tot = 0.0
+        for i in range(warmup + steps):
+            d.copy_(master)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if i >= warmup:
+                tot += e0.elapsed_time(e1)
+        return tot / steps, r
+
+    ms_plain, _ = timed(lambda: ts.sort(d.view(tdt), ctx))
+    plain_out = d.clone()
+    ms_learned, st = timed(lambda: ts.sort_learned(d.view(tdt), p, ctx))
+    ok = bool(torch.equal(d, plain_out))
+    # sortedness of the plain output as a size-independent property
+    k = plain_out.view(ibits)
+    lo = torch.iinfo(ibits).min
+    if kind != "gauss_mix_u64":  # total_cmp order of floats as signed integers
+        k = torch.where(k < 0, ~k ^ lo, k)
+    else:
+        k = k ^ lo  # unsigned order as signed
+    ok &= bool(torch.all(k[1:] >= k[:-1]).item())
+    launches0 = ts.lib().ts_ctx_launches(ctx.handle)
+    d.copy_(master)
+    ts.sort_learned(d.view(tdt), p, ctx)
+    launches = ts.lib().ts_ctx_launches(ctx.handle) - launches0
+    del master, d, plain_out, k
+    torch.cuda.empty_cache()
+    learned_bytes = n * w * 5  # predict read + partition read/write + bucket sort read/write
+    return {"gkeys_s": round(n / (ms_learned / 1e3) / 1e9, 3), "ms": round(ms_learned, 3),
+            "plain_gkeys_s": round(n / (ms_plain / 1e3) / 1e9, 3), "plain_ms": round(ms_plain, 3),
+            "speedup_vs_plain": round(ms_plain / ms_learned, 3),
+            "roofline_frac": round(learned_bytes / (ms_learned / 1e3) / 1e9 / peak, 3),
+            "fell_back": st["fell_back"], "reason": st["reason"], "imbalance": round(st["imbalance"], 3),
+            "max_bucket": st["max_bucket"], "max_cdf_error": round(st["max_cdf_error"], 5),
+            "train_loss": [st["train_loss_first"], st["train_loss_last"]],
+            "phase_ms": {k2: round(st[k2], 3) for k2 in ("ms_sample", "ms_train", "ms_partition", "ms_buckets")},
+            "launches": int(launches), "keys": n, "ok": ok,
+            "checks": "learned output == plain device sort output (bit-exact), plain output sorted"}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -558,6 +624,8 @@ def main() -> None:
         bd["c3_by_key_zipf_u64_2p27"] = bench_by_key(ts, torch, ctx, 27, max(3, args.steps // 2), 3, peak)
         for kind in ("u32", "f32"):
             bd[f"c4_segments_{kind}"] = bench_segments(ts, torch, ctx, kind, max(3, args.steps // 2), 2)
+        for kind in ("lognormal_f64", "gauss_mix_u64", "unit_f32_dups"):
+            bd[f"c5_learned_{kind}_2p28"] = bench_learned(ts, torch, ctx, kind, max(3, args.steps // 2), 3, peak)
         line["breakdown"] = bd
 
     if rank == 0:

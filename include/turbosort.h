@@ -142,6 +142,72 @@ ts_status ts_segments_methods(ts_ctx *ctx, size_t key_bytes, int *methods, int s
 /* Capture and replay CUDA graphs for repeated segmented sorts (on by default). */
 ts_status ts_ctx_use_graphs(ts_ctx *ctx, int on);
 
+/* Learned-partition sort (no counterpart in the crate; its output equals
+ * ts_sort_<T>, i.e. the crate's sort, src/dispatch.rs:31). A 1-in-sample_every
+ * sample of the keys is ranked by the plain radix sort. A two-level
+ * piecewise-linear CDF model is fitted to it on the GPU: the root puts
+ * `leaves` + 1 knots at the sample's quantiles and picks a key's leaf; each
+ * leaf is an 8-piece linear CDF over its own key range whose heights
+ * train_iters Adam steps fit to the sample's ranks (hand-written forward and
+ * backward kernels, FP32). One partition pass puts every key in one of
+ * 2^buckets_log2 buckets through the model, whose bucket map is
+ * non-decreasing in the key by construction; one segmented launch sorts every
+ * bucket. When the largest bucket exceeds overflow_factor x the mean, or the
+ * model's largest CDF error on the sample exceeds max_cdf_error, the keys take
+ * the plain sort instead (stats->fell_back = 1). use_model = 0 keeps the same
+ * partition with equal-width buckets over the key range and no model (the
+ * ablation); train_iters = 0 keeps the untrained leaves (linear in the key). */
+typedef struct ts_learned_params {
+    uint32_t buckets_log2;   /* 12..15 */
+    uint32_t sample_every;   /* sample 1 key in this many */
+    uint32_t leaves;         /* 2..2048 (with the buckets, within shared memory) */
+    uint32_t train_iters;    /* Adam steps */
+    float lr;                /* Adam step size */
+    float overflow_factor;   /* fallback when max bucket > this x mean */
+    float max_cdf_error;     /* fallback when the sample's max |CDF error| exceeds this */
+    int32_t use_model;       /* 0: equal-width buckets (ablation) */
+    uint64_t corrupt_seed;   /* test hook, 0 = off: overwrite the trained leaves with
+                                arbitrary values before the partition (output stays exact) */
+} ts_learned_params;
+
+typedef struct ts_learned_stats {
+    uint64_t n, sample_size, buckets, max_bucket;
+    double mean_bucket, imbalance;           /* imbalance = max_bucket / mean_bucket */
+    double train_loss_first, train_loss_last;  /* sample MSE before the first and after the last step */
+    float max_cdf_error;
+    uint32_t train_iters;
+    int32_t fell_back;  /* 1: the plain sort produced the output */
+    int32_t reason;     /* 1 bucket overflow, 2 CDF error, 3 input below 2^20 keys */
+    float ms_sample, ms_train, ms_partition, ms_buckets;
+} ts_learned_stats;
+
+void ts_learned_defaults(ts_learned_params *params);
+
+#define TS_DECLARE_LEARNED(SUF, T)                                                                    \
+    ts_status ts_sort_learned_##SUF(ts_ctx *ctx, T *data, size_t n, const ts_learned_params *params,   \
+                                    ts_learned_stats *stats);                                           \
+    ts_status ts_sort_learned_dev_##SUF(ts_ctx *ctx, T *d_data, size_t n, const ts_learned_params *params, \
+                                        ts_learned_stats *stats);
+
+TS_DECLARE_LEARNED(u32, uint32_t)
+TS_DECLARE_LEARNED(u64, uint64_t)
+TS_DECLARE_LEARNED(i32, int32_t)
+TS_DECLARE_LEARNED(i64, int64_t)
+TS_DECLARE_LEARNED(f32, float)
+TS_DECLARE_LEARNED(f64, double)
+
+/* The learned leaves' gradient on device arrays, for checking the backward
+ * kernel. Leaf j (of `leaves`) owns samples first[j]..last[j] (-1: none) of
+ * t[] (position in the leaf, [0, 1]) and y[] (target CDF value); its 8-piece
+ * linear CDF has interior breakpoints bp[7j .. 7j+6] and heights
+ * v[9j .. 9j+8], so prediction_i = y0[j] + h[j] * PL_j(t_i). Writes
+ * grad[9j + q] = dL/dv[9j + q] of the mean squared error
+ * L = (1/m) sum_i (prediction_i - y_i)^2, and L to *loss. A leaf whose range is
+ * not within 0..m-1 counts as empty. */
+ts_status ts_lm_gradients(ts_ctx *ctx, const float *d_t, const float *d_y, size_t m, int leaves, const int *d_first,
+                          const int *d_last, const float *d_bp, const float *d_y0, const float *d_h, const float *d_v,
+                          float *d_grad, double *loss);
+
 /* No counterpart in the reference. The device sort of u32 keys for callers
  * that cannot allocate device memory: those whose framework owns all device
  * memory and forbids raw cudaMalloc, those on latency-critical paths where an

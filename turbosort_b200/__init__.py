@@ -11,6 +11,9 @@ slices: copied to the GPU, sorted there, copied back) and CUDA torch tensors
     sort_by_key_with_buffer(items, buffer, key)   src/lib.rs:196
     SortByKeyBuffer.order() / .apply_order(other) / .capacity()   src/by_key.rs:51-145
 
+and adds the batched segmented sort (sort_segments) and the learned-partition
+sort (sort_learned), whose outputs equal the crate's sort of each slice.
+
 Every call goes through libturbosort_b200.so (include/turbosort.h); there is
 no CPU fallback: without the library or a CUDA device the calls raise.
 """
@@ -25,7 +28,7 @@ import numpy as np
 __all__ = [
     "Context", "SortByKeyBuffer", "TurbosortError", "apply_order", "default_context", "lib", "sort",
     "sort_by_key", "sort_by_key_with_buffer", "sort_parallel", "sort_segments", "sort_with_buffer", "segments_autotune",
-    "segments_methods", "TYPES",
+    "segments_methods", "TYPES", "LearnedParams", "LearnedStats", "learned_params", "lm_gradients", "sort_learned",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -47,6 +50,30 @@ STATUS = {
     1: "TS_ERR_BUFFER_TOO_SMALL", 2: "TS_ERR_LENGTH_MISMATCH", 3: "TS_ERR_CUDA", 4: "TS_ERR_TIMEOUT",
     5: "TS_ERR_OOM", 6: "TS_ERR_INVALID", 7: "TS_ERR_NO_DEVICE", 8: "TS_ERR_TOO_LARGE", 9: "TS_ERR_INTERNAL",
 }
+
+
+LEARNED_TYPES = ("u32", "u64", "i32", "i64", "f32", "f64")
+
+
+class LearnedParams(ctypes.Structure):
+    """ts_learned_params: bucket count, sample rate, model size, training and
+    fallback thresholds of the learned-partition sort."""
+    _fields_ = [("buckets_log2", ctypes.c_uint32), ("sample_every", ctypes.c_uint32), ("leaves", ctypes.c_uint32),
+                ("train_iters", ctypes.c_uint32), ("lr", ctypes.c_float), ("overflow_factor", ctypes.c_float),
+                ("max_cdf_error", ctypes.c_float), ("use_model", ctypes.c_int32), ("corrupt_seed", ctypes.c_uint64)]
+
+
+class LearnedStats(ctypes.Structure):
+    """ts_learned_stats: what the learned-partition sort did."""
+    _fields_ = [("n", ctypes.c_uint64), ("sample_size", ctypes.c_uint64), ("buckets", ctypes.c_uint64),
+                ("max_bucket", ctypes.c_uint64), ("mean_bucket", ctypes.c_double), ("imbalance", ctypes.c_double),
+                ("train_loss_first", ctypes.c_double), ("train_loss_last", ctypes.c_double),
+                ("max_cdf_error", ctypes.c_float), ("train_iters", ctypes.c_uint32), ("fell_back", ctypes.c_int32),
+                ("reason", ctypes.c_int32), ("ms_sample", ctypes.c_float), ("ms_train", ctypes.c_float),
+                ("ms_partition", ctypes.c_float), ("ms_buckets", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class TurbosortError(RuntimeError):
@@ -123,6 +150,16 @@ def lib() -> ctypes.CDLL:
             L.ts_apply_order.restype = st
             L.ts_apply_order_dev.argtypes = [vp, vp, sz, sz, vp, sz]
             L.ts_apply_order_dev.restype = st
+            for t in LEARNED_TYPES:
+                for name in ("ts_sort_learned_", "ts_sort_learned_dev_"):
+                    f = getattr(L, name + t)
+                    f.argtypes = [vp, vp, sz, ctypes.POINTER(LearnedParams), ctypes.POINTER(LearnedStats)]
+                    f.restype = st
+            L.ts_learned_defaults.argtypes = [ctypes.POINTER(LearnedParams)]
+            L.ts_learned_defaults.restype = None
+            L.ts_lm_gradients.argtypes = [vp, vp, vp, sz, i, vp, vp, vp, vp, vp, vp, vp,
+                                          ctypes.POINTER(ctypes.c_double)]
+            L.ts_lm_gradients.restype = st
             _lib = L
         return _lib
 
@@ -333,6 +370,55 @@ def segments_autotune(key_bytes: int, ctx: Context | None = None) -> list[int]:
     ctx = ctx or default_context(0)
     ctx._check(lib().ts_segments_autotune(ctx.handle, key_bytes))
     return segments_methods(key_bytes, ctx)
+
+
+def learned_params(**overrides) -> LearnedParams:
+    """The defaults of ts_learned_defaults with the given fields replaced."""
+    p = LearnedParams()
+    lib().ts_learned_defaults(ctypes.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise TypeError(f"no learned-sort parameter {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+def sort_learned(a, params: LearnedParams | None = None, ctx: Context | None = None, **overrides) -> dict:
+    """Sort `a` in place through the learned partition (same output as
+    `sort`); returns the run's statistics (imbalance, training loss, whether it
+    fell back to the plain sort, per-phase milliseconds)."""
+    ctx = ctx or default_context(a.device.index if _is_torch(a) else 0)
+    t = _type_of(a)
+    if t not in LEARNED_TYPES:
+        raise TypeError(f"the learned sort takes {', '.join(LEARNED_TYPES)} keys, not {t}")
+    p = params if params is not None else learned_params(**overrides)
+    st = LearnedStats()
+    if _dev(a):
+        ctx._check(getattr(lib(), f"ts_sort_learned_dev_{t}")(ctx.handle, a.data_ptr(), a.numel(), ctypes.byref(p),
+                                                              ctypes.byref(st)))
+    else:
+        ctx._check(getattr(lib(), f"ts_sort_learned_{t}")(ctx.handle, _host_ptr(a), a.size, ctypes.byref(p),
+                                                          ctypes.byref(st)))
+    return st.as_dict()
+
+
+LM_PIECES = 8  # pieces of every leaf's linear CDF
+
+
+def lm_gradients(t, y, first, last, bp, y0, h, v, ctx: Context | None = None):
+    """The learned leaves' backward kernel on CUDA tensors: returns (dL/dv, L)
+    for L = mean_i (y0[j] + h[j] * PL_j(t_i) - y_i)^2, leaf j owning samples
+    first[j]..last[j]; bp is [leaves, 7] (interior breakpoints), v is
+    [leaves, 9] (heights); the gradient has v's shape."""
+    import torch
+    ctx = ctx or default_context(t.device.index)
+    leaves = y0.numel()
+    grad = torch.empty((leaves, LM_PIECES + 1), dtype=torch.float32, device=t.device)
+    loss = ctypes.c_double(0.0)
+    ctx._check(lib().ts_lm_gradients(ctx.handle, t.data_ptr(), y.data_ptr(), t.numel(), leaves, first.data_ptr(),
+                                     last.data_ptr(), bp.data_ptr(), y0.data_ptr(), h.data_ptr(), v.data_ptr(),
+                                     grad.data_ptr(), ctypes.byref(loss)))
+    return grad, loss.value
 
 
 def _key_array(items, key, dtype):

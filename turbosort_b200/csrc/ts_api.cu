@@ -230,7 +230,7 @@ void ts_ctx_destroy(ts_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg})
+    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg, &c->learn})
         if (b->p) cudaFree(b->p);
     if (c->seg_graph) cudaGraphExecDestroy(c->seg_graph);
     if (c->d_error) cudaFree(c->d_error);

@@ -36,6 +36,7 @@ struct ts_ctx {
     ts::DevBuf lookback;           // two look-back regions
     ts::DevBuf gather;             // apply_order staging
     ts::DevBuf seg;                // segmented sort: plan, work counter, bin lists, offsets
+    ts::DevBuf learn;              // learned partition: sample, model, training state, bucket counts
     uint32_t* d_error = nullptr;   // kernel-reported errors, read and cleared by the host
 
     // segmented sort: the method of each on-chip length bin per key width

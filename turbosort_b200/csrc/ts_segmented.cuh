@@ -90,8 +90,8 @@ static __global__ void k_seg_items(SegPlan* plan) {
 
 // ---- WARP: bitonic network over 32 lanes ---------------------------------
 template <typename U, int XF>
-__device__ __forceinline__ void seg_warp_sort(U* seg, int len, int lane) {
-    U v = lane < len ? to_key<U, XF>(seg[lane]) : (U)~(U)0;
+__device__ __forceinline__ void seg_warp_sort(const U* in, U* seg, int len, int lane) {
+    U v = lane < len ? to_key<U, XF>(in[lane]) : (U)~(U)0;
 #pragma unroll
     for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
@@ -107,10 +107,10 @@ __device__ __forceinline__ void seg_warp_sort(U* seg, int len, int lane) {
 // ---- BLOCK: on-chip sorts ---------------------------------------------------
 // Bitonic over the next power of two in shared memory.
 template <typename U, int XF>
-__device__ void seg_block_bitonic(U* seg, int len, U* sm) {
+__device__ void seg_block_bitonic(const U* in, U* seg, int len, U* sm) {
     int p2 = 1;
     while (p2 < len) p2 <<= 1;
-    for (int i = threadIdx.x; i < p2; i += SEG_THREADS) sm[i] = i < len ? to_key<U, XF>(seg[i]) : (U)~(U)0;
+    for (int i = threadIdx.x; i < p2; i += SEG_THREADS) sm[i] = i < len ? to_key<U, XF>(in[i]) : (U)~(U)0;
     __syncthreads();
     for (int k = 2; k <= p2; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
@@ -195,7 +195,8 @@ __device__ __forceinline__ void seg_rank_pass(const U (&k)[IPT], int wbase, int 
 }
 
 template <typename U, int XF, int BITS>
-__device__ void seg_block_radix(U* seg, int len, U* sm, uint32_t* cnt, int* warp_tot, unsigned long long* red) {
+__device__ void seg_block_radix(const U* in, U* seg, int len, U* sm, uint32_t* cnt, int* warp_tot,
+                                unsigned long long* red) {
     constexpr int IPT = SegCfg<U>::IPT;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -208,12 +209,12 @@ __device__ void seg_block_radix(U* seg, int len, U* sm, uint32_t* cnt, int* warp
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
         const int idx = wbase + i * 32;
-        k[i] = (i < ipt && idx < len) ? to_key<U, XF>(seg[idx]) : (U)0;
+        k[i] = (i < ipt && idx < len) ? to_key<U, XF>(in[idx]) : (U)0;
     }
     if (threadIdx.x == 0) *red = 0;
     __syncthreads();
     // the bits in which some key differs from the first: only those digits get a pass
-    const U first = to_key<U, XF>(seg[0]);
+    const U first = to_key<U, XF>(in[0]);
     unsigned long long d = 0;
 #pragma unroll
     for (int i = 0; i < IPT; ++i)
@@ -259,8 +260,8 @@ struct SegSmem {
 };
 
 template <typename U, int XF>
-__device__ void seg_large_sort(U* seg, U* alt, int len, U* sm, uint32_t* cnt, int* warp_tot, unsigned long long* red,
-                               uint32_t* hist, uint32_t* run, uint32_t* lst, uint32_t* tcnt) {
+__device__ void seg_large_sort(const U* in, U* seg, U* alt, int len, U* sm, uint32_t* cnt, int* warp_tot,
+                               unsigned long long* red, uint32_t* hist, uint32_t* run, uint32_t* lst, uint32_t* tcnt) {
     constexpr int RADIX = 256;
     constexpr int ND = (int)sizeof(U);
     constexpr int IPT = SegCfg<U>::LARGE_IPT;
@@ -272,10 +273,10 @@ __device__ void seg_large_sort(U* seg, U* alt, int len, U* sm, uint32_t* cnt, in
     for (int i = tid; i < ND * RADIX; i += SEG_THREADS) hist[i] = 0;
     if (tid == 0) *red = 0;
     __syncthreads();
-    const U first = to_key<U, XF>(seg[0]);
+    const U first = to_key<U, XF>(in[0]);
     unsigned long long d = 0;
     for (int i = tid; i < len; i += SEG_THREADS) {
-        const U k = to_key<U, XF>(seg[i]);
+        const U k = to_key<U, XF>(in[i]);
         d |= (unsigned long long)(k ^ first);
 #pragma unroll
         for (int p = 0; p < ND; ++p) atomicAdd(&hist[p * RADIX + digit_of(k, p * 8, RADIX - 1)], 1u);
@@ -292,7 +293,7 @@ __device__ void seg_large_sort(U* seg, U* alt, int len, U* sm, uint32_t* cnt, in
     bool in_alt = false, first_pass = true;
     for (int p = 0; p < ND; ++p) {
         if (((vary >> (p * 8)) & 0xff) == 0) continue;
-        const U* src = in_alt ? alt : seg;
+        const U* src = first_pass ? in : (in_alt ? alt : seg);
         U* dst = in_alt ? seg : alt;
         const bool last = p == last_p;
         // exclusive scan of this digit's histogram into run[]
@@ -339,6 +340,8 @@ __device__ void seg_large_sort(U* seg, U* alt, int len, U* sm, uint32_t* cnt, in
     }
     if (in_alt) {
         for (int i = tid; i < len; i += SEG_THREADS) seg[i] = alt[i];
+    } else if (first_pass && in != seg) {  // every key equal: nothing moved yet
+        for (int i = tid; i < len; i += SEG_THREADS) seg[i] = in[i];
     }
 }
 
@@ -349,7 +352,7 @@ struct SegMethods {
 
 template <typename U, int XF>
 __global__ void __launch_bounds__(SEG_THREADS, 1)
-    k_seg_sort(U* __restrict__ data, U* __restrict__ alt, const unsigned long long* __restrict__ offsets,
+    k_seg_sort(const U* data_in, U* data, U* __restrict__ alt, const unsigned long long* __restrict__ offsets,
                const unsigned int* __restrict__ lists, size_t n_seg, const SegPlan* __restrict__ plan,
                unsigned int* __restrict__ counter, SegMethods methods) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -379,19 +382,20 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
             if (idx < plan->count[SEG_BIN_WARP]) {
                 const unsigned int s = lists[(size_t)SEG_BIN_WARP * n_seg + idx];
                 const unsigned long long b = offsets[s];
-                seg_warp_sort<U, XF>(data + b, (int)(offsets[s + 1] - b), lane);
+                seg_warp_sort<U, XF>(data_in + b, data + b, (int)(offsets[s + 1] - b), lane);
             }
         } else {
             const unsigned int s = lists[(size_t)bin * n_seg + first];
             const unsigned long long b = offsets[s];
             const int len = (int)(offsets[s + 1] - b);
             if (bin == SEG_BIN_LARGE) {
-                seg_large_sort<U, XF>(data + b, alt + b, len, sm, cnt, warp_tot, red, hist, run, lst, tcnt);
+                seg_large_sort<U, XF>(data_in + b, data + b, alt + b, len, sm, cnt, warp_tot, red, hist, run, lst,
+                                      tcnt);
             } else {
                 const int m = methods.m[bin];
-                if (m == SEG_BITONIC) seg_block_bitonic<U, XF>(data + b, len, sm);
-                else if (m == SEG_RADIX4) seg_block_radix<U, XF, 4>(data + b, len, sm, cnt, warp_tot, red);
-                else seg_block_radix<U, XF, 8>(data + b, len, sm, cnt, warp_tot, red);
+                if (m == SEG_BITONIC) seg_block_bitonic<U, XF>(data_in + b, data + b, len, sm);
+                else if (m == SEG_RADIX4) seg_block_radix<U, XF, 4>(data_in + b, data + b, len, sm, cnt, warp_tot, red);
+                else seg_block_radix<U, XF, 8>(data_in + b, data + b, len, sm, cnt, warp_tot, red);
             }
         }
         __syncthreads();

@@ -70,8 +70,8 @@ ts_status seg_enqueue(ts_ctx* c, U* d, size_t n, const unsigned long long* d_off
     const int grid = (int)std::min<size_t>((n_seg + 255) / 256, (size_t)c->sm_count * 8);
     k_seg_bin_max<U, XF><<<std::max(grid, 1), 256, 0, c->stream>>>(d_off, n_seg, n, max_len, plan, lists, c->d_error);
     k_seg_items<<<1, 32, 0, c->stream>>>(plan);
-    k_seg_sort<U, XF><<<c->sm_count, SEG_THREADS, SegSmem::bytes<U>(), c->stream>>>(d, (U*)c->alt.p, d_off, lists,
-                                                                                     n_seg, plan, counter, m);
+    k_seg_sort<U, XF><<<c->sm_count, SEG_THREADS, SegSmem::bytes<U>(), c->stream>>>(d, d, (U*)c->alt.p, d_off,
+                                                                                     lists, n_seg, plan, counter, m);
     c->launches += 3;
     TS_CUDA(c, cudaGetLastError());
     return TS_OK;
