@@ -162,7 +162,7 @@ typedef struct ts_learned_params {
     uint32_t sample_every;   /* sample 1 key in this many */
     uint32_t leaves;         /* 2..2048 (with the buckets, within shared memory) */
     uint32_t train_iters;    /* Adam steps */
-    float lr;                /* Adam step size */
+    float lr;                /* Adam step size, as a fraction of each leaf's initial RMS rank error */
     float overflow_factor;   /* fallback when max bucket > this x mean */
     float max_cdf_error;     /* fallback when the sample's max |CDF error| exceeds this */
     int32_t use_model;       /* 0: equal-width buckets (ablation) */

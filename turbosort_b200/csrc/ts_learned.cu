@@ -135,12 +135,14 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
                                     LM_FIN_SMEM));
 
     Events ev;
+    mark(c, "lm_sample");
     cudaEventRecord(ev.e[0], c->stream);
     // 1. sample, and its exact ranks from the plain radix sort
     U* sample = (U*)B.sample;
     k_lm_sample<U><<<c->sm_count * 4, 256, 0, c->stream>>>(d, n, every, sample, m, XF);
     ++c->launches;
     if ((s = sort_keys_device<U, 0>(c, sample, m, nullptr)) != TS_OK) return done(s);
+    mark(c, "lm_fit");
     TS_CUDA(c, cudaMemsetAsync(B.T.first, 0xff, (size_t)leaves * 4, c->stream));
     TS_CUDA(c, cudaMemsetAsync(B.T.last, 0xff, (size_t)leaves * 4, c->stream));
     TS_CUDA(c, cudaMemsetAsync(B.loss, 0, 2 * 8, c->stream));
@@ -168,6 +170,7 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     }
     cudaEventRecord(ev.e[2], c->stream);
     // 3. every key's bucket, the bucket sizes and offsets, the largest bucket
+    mark(c, "lm_count");
     const int count_grid = std::max<int>(1, std::min<int>(c->sm_count, (int)((n + 4095) / 4096)));
     k_lm_count<U, XF><<<count_grid, 1024, count_smem, c->stream>>>(d, n, B.head, B.T, ids, B.totals);
     k_lm_bucket_scan<<<1, 1024, 0, c->stream>>>(B.totals, buckets, B.offsets, B.max_bucket, B.cur1, B.cur2,
@@ -217,12 +220,15 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     U* part = (U*)c->alt.p;
     U* grouped = (U*)c->gather.p;
     const int split_tiles = (int)((n + LM_SPLIT_TILE - 1) / LM_SPLIT_TILE);
+    mark(c, "lm_split");
     cudaEventRecord(ev.e[4], c->stream);
-    k_lm_split1<U><<<split_tiles, 1024, LmSplitSmem<U>::bytes, c->stream>>>(d, ids, n, blog - 7, B.cur1, B.offsets,
-                                                                            grouped, ids1, c->d_error);
-    k_lm_split2<U><<<split_tiles + LM_SUPERS, 1024, LmSplitSmem<U>::bytes, c->stream>>>(
-        grouped, ids1, buckets, B.offsets, B.tiles_before, B.cur2, part, c->d_error);
+    const int split_grid = std::min(split_tiles, c->sm_count);
+    k_lm_split1<U><<<split_grid, 1024, LmSplitSmem<U>::bytes, c->stream>>>(d, ids, n, blog - 7, B.cur1, B.offsets,
+                                                                           grouped, ids1, c->d_error);
+    k_lm_split2<U><<<c->sm_count, 1024, LmSplitSmem<U>::bytes, c->stream>>>(grouped, ids1, buckets, B.offsets,
+                                                                           B.tiles_before, B.cur2, part, c->d_error);
     c->launches += 2;
+    mark(c, "lm_finish");
     cudaEventRecord(ev.e[5], c->stream);
     k_lm_finish<U, XF><<<c->sm_count, 1024, LM_FIN_SMEM, c->stream>>>(part, d, grouped, B.offsets, buckets, B.counter);
     ++c->launches;
@@ -260,7 +266,7 @@ void ts_learned_defaults(ts_learned_params* p) {
     p->sample_every = 100;
     p->leaves = 1024;
     p->train_iters = 32;
-    p->lr = 0.05f;
+    p->lr = 0.5f;
     p->overflow_factor = 4.f;
     p->max_cdf_error = 0.01f;
     p->use_model = 1;

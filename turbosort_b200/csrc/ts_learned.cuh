@@ -290,8 +290,9 @@ __device__ void lm_leaf_grads(int f, int l, const float* bp, const float* pv, fl
 // Training: one CTA per leaf (a leaf's heights only enter its own samples'
 // terms of the loss, so leaves train independently), every Adam step on chip.
 // Adam sees dL/dv scaled by m / (2 h^2), a per-leaf constant, which leaves its
-// steps unchanged and keeps them clear of its epsilon; the step size decays
-// linearly to zero. Reports the loss before the first step and after the
+// steps unchanged and keeps them clear of its epsilon. The step size is lr
+// times the leaf's initial RMS rank error (in leaf units) and decays linearly
+// to zero. Reports the loss before the first step and after the
 // last, and the largest |rank error| after the last.
 template <typename U>
 __global__ void __launch_bounds__(LM_TRAIN_THREADS) k_lm_train(const U* __restrict__ s, size_t m, LmTables T,
@@ -316,10 +317,14 @@ __global__ void __launch_bounds__(LM_TRAIN_THREADS) k_lm_train(const U* __restri
     float g[LM_P + 1];
     float sse = 0.f, emax = 0.f;
     const float b1 = 0.9f, b2 = 0.999f;
+    __shared__ float rms0;  // the leaf's RMS rank error before training, in leaf units
     for (int it = 0; it < iters; ++it) {
         lm_leaf_grads(f, l, bp, pv, y0, h, inv_m, t_of, y_of, g_red, e_red, g, sse, emax);
         if (threadIdx.x == 0) {
-            if (it == 0) atomicAdd(loss_first, (double)sse / (double)m);
+            if (it == 0) {
+                atomicAdd(loss_first, (double)sse / (double)m);
+                rms0 = h > 0.f ? sqrtf(sse / (float)(l - f + 1)) / h : 0.f;
+            }
 #pragma unroll
             for (int q = 0; q <= LM_P; ++q) g_red[q] = g[q];  // hand the gradient to threads 0..P
         }
@@ -329,7 +334,9 @@ __global__ void __launch_bounds__(LM_TRAIN_THREADS) k_lm_train(const U* __restri
             m1 = b1 * m1 + (1.f - b1) * gq;
             m2 = b2 * m2 + (1.f - b2) * gq * gq;
             const float c1 = 1.f - __powf(b1, (float)(it + 1)), c2 = 1.f - __powf(b2, (float)(it + 1));
-            const float step = lr * (1.f - (float)it / (float)iters);
+            // steps start at lr x the leaf's RMS error (the scale of the corrections
+            // it needs) and decay linearly to zero
+            const float step = lr * rms0 * (1.f - (float)it / (float)iters);
             pv[threadIdx.x] -= step * (m1 / c1) / (sqrtf(m2 / c2) + 1e-8f);
         }
         __syncthreads();
@@ -692,7 +699,19 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
     __syncthreads();
 }
 
+// Starts an asynchronous copy of global bytes [begin, end) into L2, narrowed
+// to 16-byte bounds (the bulk prefetch's rule), so it never touches a byte
+// outside the range.
+__device__ __forceinline__ void lm_prefetch_l2(const void* begin, const void* end) {
+    const uintptr_t a = ((uintptr_t)begin + 15) & ~(uintptr_t)15;
+    const uintptr_t e = (uintptr_t)end & ~(uintptr_t)15;
+    if (e > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
 // First sweep: keys (and ids) into LM_SUPERS groups of consecutive buckets.
+// Persistent CTAs take every gridDim.x-th tile and prefetch the next one into
+// L2 while they work on the current one.
 template <typename U>
 __global__ void __launch_bounds__(1024, 1) k_lm_split1(const U* __restrict__ src, const unsigned short* __restrict__ ids,
                                                        size_t n, int shift, unsigned long long* __restrict__ cur1,
@@ -700,15 +719,39 @@ __global__ void __launch_bounds__(1024, 1) k_lm_split1(const U* __restrict__ src
                                                        U* __restrict__ dst, unsigned short* __restrict__ dst_ids,
                                                        uint32_t* __restrict__ error) {
     extern __shared__ __align__(16) unsigned char ssm[];
-    const size_t t0 = (size_t)blockIdx.x * LM_SPLIT_TILE;
-    if (t0 >= n) return;
-    const int len = (int)min((size_t)LM_SPLIT_TILE, n - t0);
-    lm_split_tile<U, true>(src + t0, ids + t0, len, shift, LM_SUPERS, cur1, offsets, 1 << shift, dst, dst_ids, ssm,
-                           error);
+    const size_t tiles = (n + LM_SPLIT_TILE - 1) / LM_SPLIT_TILE;
+    for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const size_t t0 = tile * LM_SPLIT_TILE;
+        const int len = (int)min((size_t)LM_SPLIT_TILE, n - t0);
+        if (threadIdx.x == 0 && tile + gridDim.x < tiles) {
+            const size_t u0 = t0 + (size_t)gridDim.x * LM_SPLIT_TILE, u1 = min(n, u0 + LM_SPLIT_TILE);
+            lm_prefetch_l2(src + u0, src + u1);
+            lm_prefetch_l2(ids + u0, ids + u1);
+        }
+        lm_split_tile<U, true>(src + t0, ids + t0, len, shift, LM_SUPERS, cur1, offsets, 1 << shift, dst, dst_ids, ssm,
+                               error);
+    }
 }
 
-// Second sweep: inside each group, keys to their buckets. Tiles never cross
-// a group's boundary (tiles_before[] numbers them group by group).
+// The second sweep's tile number `tile` as (group S, start, length); tiles
+// never cross a group's boundary (tiles_before[] numbers them group by group).
+__device__ __forceinline__ int lm_tile2(unsigned int tile, int per, const unsigned long long* __restrict__ offsets,
+                                        const unsigned int* __restrict__ tiles_before, unsigned long long& t0,
+                                        int& len) {
+    int lo = 0, hi = LM_SUPERS - 1;  // the group S with tiles_before[S] <= tile < tiles_before[S + 1]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tiles_before[mid] <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    const unsigned long long g0 = offsets[lo * per], g1 = offsets[(lo + 1) * per];
+    t0 = g0 + (unsigned long long)(tile - tiles_before[lo]) * LM_SPLIT_TILE;
+    len = t0 < g1 ? (int)min((unsigned long long)LM_SPLIT_TILE, g1 - t0) : 0;
+    return lo;
+}
+
+// Second sweep: inside each group, keys to their buckets; persistent CTAs
+// with the next tile prefetched into L2, as in the first sweep.
 template <typename U>
 __global__ void __launch_bounds__(1024, 1) k_lm_split2(const U* __restrict__ src, const unsigned short* __restrict__ ids,
                                                        int buckets, const unsigned long long* __restrict__ offsets,
@@ -716,22 +759,23 @@ __global__ void __launch_bounds__(1024, 1) k_lm_split2(const U* __restrict__ src
                                                        unsigned long long* __restrict__ cur2, U* __restrict__ dst,
                                                        uint32_t* __restrict__ error) {
     extern __shared__ __align__(16) unsigned char ssm[];
-    const unsigned int tile = blockIdx.x;
-    if (tile >= tiles_before[LM_SUPERS]) return;
-    int lo = 0, hi = LM_SUPERS - 1;  // the group S with tiles_before[S] <= tile < tiles_before[S + 1]
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tiles_before[mid] <= tile) lo = mid;
-        else hi = mid - 1;
-    }
-    const int S = lo;
+    const unsigned int tiles = tiles_before[LM_SUPERS];
     const int per = buckets / LM_SUPERS;
-    const unsigned long long g0 = offsets[S * per], g1 = offsets[(S + 1) * per];
-    const unsigned long long t0 = g0 + (unsigned long long)(tile - tiles_before[S]) * LM_SPLIT_TILE;
-    if (t0 >= g1) return;
-    const int len = (int)min((unsigned long long)LM_SPLIT_TILE, g1 - t0);
-    lm_split_tile<U, false>(src + t0, ids + t0, len, 0, per, cur2 + (size_t)S * per, offsets + (size_t)S * per, 1, dst,
-                            nullptr, ssm, error);
+    for (unsigned int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        unsigned long long t0;
+        int len;
+        const int S = lm_tile2(tile, per, offsets, tiles_before, t0, len);
+        if (threadIdx.x == 0 && tile + gridDim.x < tiles) {
+            unsigned long long u0;
+            int ulen;
+            lm_tile2(tile + gridDim.x, per, offsets, tiles_before, u0, ulen);
+            lm_prefetch_l2(src + u0, src + u0 + ulen);
+            lm_prefetch_l2(ids + u0, ids + u0 + ulen);
+        }
+        if (len > 0)  // uniform over the CTA
+            lm_split_tile<U, false>(src + t0, ids + t0, len, 0, per, cur2 + (size_t)S * per, offsets + (size_t)S * per,
+                                    1, dst, nullptr, ssm, error);
+    }
 }
 
 // ---- bucket finish -----------------------------------------------------------
@@ -745,6 +789,27 @@ __global__ void __launch_bounds__(1024, 1) k_lm_split2(const U* __restrict__ src
 constexpr int LM_FIN_SMEM = 200 * 1024;
 constexpr int LM_SUB_BITS = 11;
 constexpr int LM_SUB_MAX = 64;
+
+// fn(i, src[i]) for this thread's share of 0..len-1, its loads issued a
+// group at a time (one bucket is read by one CTA: latency, not bandwidth,
+// bounds a plain loop)
+template <typename U, typename Fn>
+__device__ __forceinline__ void lm_for_keys(const U* __restrict__ src, int len, Fn fn) {
+    constexpr int G = 32 / sizeof(U);
+    for (int base = threadIdx.x; base < len; base += 1024 * G) {
+        U v[G];
+#pragma unroll
+        for (int e = 0; e < G; ++e) {
+            const int i = base + e * 1024;
+            v[e] = i < len ? src[i] : (U)0;
+        }
+#pragma unroll
+        for (int e = 0; e < G; ++e) {
+            const int i = base + e * 1024;
+            if (i < len) fn(i, v[e]);
+        }
+    }
+}
 
 template <typename U>
 struct LmFinSmem {
@@ -773,11 +838,21 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
     uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
     uint32_t* l_run = l_hist + 8 * 256;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) red[2] = 0ull;
+    if (tid == 0) {
+        red[2] = 0ull;
+        item_s[1] = (int)atomicAdd(counter, 1u);
+    }
     for (;;) {
-        if (tid == 0) *item_s = (int)atomicAdd(counter, 1u);
+        // take the bucket claimed last time, claim the next one and start
+        // bringing it into L2 while this one is sorted
+        if (tid == 0) {
+            item_s[0] = item_s[1];
+            const int nb = (int)atomicAdd(counter, 1u);
+            item_s[1] = nb;
+            if (nb < buckets) lm_prefetch_l2(in + offsets[nb], in + offsets[nb + 1]);
+        }
         __syncthreads();
-        const int b = *item_s;
+        const int b = item_s[0];
         __syncthreads();
         if (b >= buckets) break;
         const unsigned long long lo = offsets[b];
@@ -799,11 +874,11 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
             }
             __syncthreads();
             unsigned long long mn = ~0ull, mx = 0ull;
-            for (int i = tid; i < len; i += 1024) {
-                const unsigned long long k = (unsigned long long)to_key<U, XF>(src[i]);
+            lm_for_keys<U>(src, len, [&](int, U v) {
+                const unsigned long long k = (unsigned long long)to_key<U, XF>(v);
                 mn = k < mn ? k : mn;
                 mx = k > mx ? k : mx;
-            }
+            });
             for (int o = 16; o > 0; o >>= 1) {
                 const unsigned long long a = __shfl_xor_sync(0xffffffffu, mn, o);
                 const unsigned long long c = __shfl_xor_sync(0xffffffffu, mx, o);
@@ -818,7 +893,7 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
             kmin = red[0];
             kmax = red[1];
             if (kmin == kmax) {  // every key equal
-                for (int i = tid; i < len; i += 1024) dst[i] = src[i];
+                lm_for_keys<U>(src, len, [&](int i, U v) { dst[i] = v; });
                 __syncthreads();
                 continue;
             }
@@ -832,7 +907,8 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
             // pass 2: counts per sub-range, their starts, the largest
             for (int d = tid; d < nb; d += 1024) hist[d] = 0;
             __syncthreads();
-            for (int i = tid; i < len; i += 1024) atomicAdd(&hist[digit((unsigned long long)to_key<U, XF>(src[i]))], 1u);
+            lm_for_keys<U>(src, len,
+                           [&](int, U v) { atomicAdd(&hist[digit((unsigned long long)to_key<U, XF>(v))], 1u); });
             __syncthreads();
             unsigned int v0 = 2 * tid < nb ? hist[2 * tid] : 0u, v1 = 2 * tid + 1 < nb ? hist[2 * tid + 1] : 0u;
             unsigned int x = v0 + v1, m = max(v0, v1);
@@ -864,10 +940,10 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
         // pass 3: place keys by sub-range (cursor = hist, reset to the starts)
         for (int d = tid; d < nb; d += 1024) hist[d] = start[d];
         __syncthreads();
-        for (int i = tid; i < len; i += 1024) {
-            const U k = to_key<U, XF>(src[i]);
+        lm_for_keys<U>(src, len, [&](int, U v) {
+            const U k = to_key<U, XF>(v);
             sk[atomicAdd(&hist[digit((unsigned long long)k)], 1u)] = k;
-        }
+        });
         __syncthreads();
         // pass 4: every sub-range sorted by one thread
         for (int d = tid; d < nb; d += 1024) {
