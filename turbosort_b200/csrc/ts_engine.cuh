@@ -29,8 +29,12 @@ struct LsdCfg {
     // per-warp counters) share one SM's shared memory
     static constexpr int IPT = sizeof(U) == 8 ? 7 : (PAIRS ? 11 : (sizeof(U) == 4 ? 15 : 16));
     static constexpr int NBUF = PAIRS ? 1 : 2;  // tiles of keys in flight per CTA
-    static constexpr int MATCH_MOD = 4;         // items with i % MATCH_MOD < MATCH_CNT use match.any
-    static constexpr int MATCH_CNT = 0;
+    // items with i % MATCH_MOD < MATCH_CNT find their digit's peers with
+    // match.any, the rest with ballots: one item in four keeps the match unit
+    // busy without making it the bottleneck and takes a quarter of the ranking
+    // off the integer pipe (2^28 u32 keys on a B200: 5.81 -> 5.19 ms a sort)
+    static constexpr int MATCH_MOD = 4;
+    static constexpr int MATCH_CNT = 1;
     using Smem = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
     static constexpr int TILE = Smem::TILE;
     static constexpr int RADIX = 1 << BITS;

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_onesweep(SweepArgs<U, PAIRS> a) 
         const size_t tile_base = a.portion_begin + (size_t)t * TILE;
         const int tile_n = FULL ? TILE : (int)min((size_t)TILE, portion_end - tile_base);
         U* kb = kbuf + (size_t)b * TILE;
-        uint32_t* vb = vbuf + (size_t)b * TILE;
+        [[maybe_unused]] uint32_t* vb = vbuf + (size_t)b * TILE;
 
         // ---- 1. the tile's keys in shared memory
         if (!mbar_wait(&bars[b], (parity >> b) & 1u)) atomicOr(a.error, ERR_TIMEOUT);
@@ -310,21 +310,37 @@ __global__ void __launch_bounds__(THREADS, 2) k_onesweep(SweepArgs<U, PAIRS> a) 
                 const int r = tid * DPT + q;
                 uint32_t excl = 0;
                 if (t > 0) {
+                    // LB_WINDOW predecessors per round trip: their loads go out
+                    // together, then they are summed newest first up to the
+                    // first inclusive entry; an entry not yet published ends
+                    // the round there and the next round starts from it
                     int j = t - 1;
                     uint32_t spins = 0;
-                    while (j >= 0) {
-                        const uint32_t w = ld_relaxed_gpu(a.lookback + (size_t)j * RADIX + r);
-                        const uint32_t f = w & ~LB_VALUE;
-                        if (f == 0) {
-                            if (++spins > SPIN_LIMIT) {
-                                atomicOr(a.error, ERR_TIMEOUT);
-                                break;
+                    bool done = false;
+                    while (j >= 0 && !done) {
+                        uint32_t w[LB_WINDOW];
+#pragma unroll
+                        for (int k = 0; k < LB_WINDOW; ++k)
+                            w[k] = j - k >= 0 ? ld_relaxed_gpu(a.lookback + (size_t)(j - k) * RADIX + r) : LB_FLAG_INC;
+                        int adv = 0;
+                        bool stalled = false;
+#pragma unroll
+                        for (int k = 0; k < LB_WINDOW; ++k) {
+                            const uint32_t f = w[k] & ~LB_VALUE;
+                            if (done || stalled) continue;
+                            if (f == 0) {
+                                stalled = true;
+                                continue;
                             }
-                            continue;
+                            excl += w[k] & LB_VALUE;
+                            ++adv;
+                            if (f == LB_FLAG_INC) done = true;
                         }
-                        excl += w & LB_VALUE;
-                        if (f == LB_FLAG_INC) break;
-                        --j;
+                        j -= adv;
+                        if (adv == 0 && ++spins > SPIN_LIMIT) {
+                            atomicOr(a.error, ERR_TIMEOUT);
+                            break;
+                        }
                     }
                     st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, LB_FLAG_INC | (excl + tcount[q]));
                 }
