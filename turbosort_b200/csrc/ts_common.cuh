@@ -130,6 +130,16 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, u
         "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
+// Starts an asynchronous copy of global bytes [begin, end) into L2, narrowed
+// to 16-byte bounds (the bulk prefetch's rule), so it never touches a byte
+// outside the range.
+__device__ __forceinline__ void prefetch_l2(const void* begin, const void* end) {
+    const uintptr_t a = ((uintptr_t)begin + 15) & ~(uintptr_t)15;
+    const uintptr_t e = (uintptr_t)end & ~(uintptr_t)15;
+    if (e > a)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
 // Bounded wait on an mbarrier phase; returns false if the limit ran out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
     uint32_t ok = 0;

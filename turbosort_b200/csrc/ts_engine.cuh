@@ -25,10 +25,13 @@ template <typename U, bool PAIRS>
 struct LsdCfg {
     static constexpr int BITS = 8;
     static constexpr int THREADS = 512;
-    // sized so that two CTAs (double-buffered keys, staging tile, 32-bit
-    // per-warp counters) share one SM's shared memory
-    static constexpr int IPT = sizeof(U) == 8 ? 7 : (PAIRS ? 11 : (sizeof(U) == 4 ? 15 : 16));
-    static constexpr int NBUF = PAIRS ? 1 : 2;  // tiles of keys in flight per CTA
+    // the largest tile for which two CTAs (one tile of keys and positions, the
+    // staging tile, 32-bit per-warp counters) share one SM's shared memory:
+    // the per-tile costs (look-back, counter scans) shrink per key as tiles
+    // grow, which on a B200 outweighs double-buffering a smaller tile
+    // (2^28 u32 keys: 15 keys a thread double-buffered 5.18 ms, 22 single 4.83 ms)
+    static constexpr int IPT = sizeof(U) == 8 ? (PAIRS ? 7 : 11) : (PAIRS ? 11 : (sizeof(U) == 4 ? 22 : 32));
+    static constexpr int NBUF = 1;  // tiles of keys in flight per CTA; the next one is prefetched into L2
     // items with i % MATCH_MOD < MATCH_CNT find their digit's peers with
     // match.any, the rest with ballots: one item in four keeps the match unit
     // busy without making it the bottleneck and takes a quarter of the ranking

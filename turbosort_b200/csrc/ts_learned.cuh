@@ -699,16 +699,6 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
     __syncthreads();
 }
 
-// Starts an asynchronous copy of global bytes [begin, end) into L2, narrowed
-// to 16-byte bounds (the bulk prefetch's rule), so it never touches a byte
-// outside the range.
-__device__ __forceinline__ void lm_prefetch_l2(const void* begin, const void* end) {
-    const uintptr_t a = ((uintptr_t)begin + 15) & ~(uintptr_t)15;
-    const uintptr_t e = (uintptr_t)end & ~(uintptr_t)15;
-    if (e > a)
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
-}
-
 // First sweep: keys (and ids) into LM_SUPERS groups of consecutive buckets.
 // Persistent CTAs take every gridDim.x-th tile and prefetch the next one into
 // L2 while they work on the current one.
@@ -725,8 +715,8 @@ __global__ void __launch_bounds__(1024, 1) k_lm_split1(const U* __restrict__ src
         const int len = (int)min((size_t)LM_SPLIT_TILE, n - t0);
         if (threadIdx.x == 0 && tile + gridDim.x < tiles) {
             const size_t u0 = t0 + (size_t)gridDim.x * LM_SPLIT_TILE, u1 = min(n, u0 + LM_SPLIT_TILE);
-            lm_prefetch_l2(src + u0, src + u1);
-            lm_prefetch_l2(ids + u0, ids + u1);
+            prefetch_l2(src + u0, src + u1);
+            prefetch_l2(ids + u0, ids + u1);
         }
         lm_split_tile<U, true>(src + t0, ids + t0, len, shift, LM_SUPERS, cur1, offsets, 1 << shift, dst, dst_ids, ssm,
                                error);
@@ -769,8 +759,8 @@ __global__ void __launch_bounds__(1024, 1) k_lm_split2(const U* __restrict__ src
             unsigned long long u0;
             int ulen;
             lm_tile2(tile + gridDim.x, per, offsets, tiles_before, u0, ulen);
-            lm_prefetch_l2(src + u0, src + u0 + ulen);
-            lm_prefetch_l2(ids + u0, ids + u0 + ulen);
+            prefetch_l2(src + u0, src + u0 + ulen);
+            prefetch_l2(ids + u0, ids + u0 + ulen);
         }
         if (len > 0)  // uniform over the CTA
             lm_split_tile<U, false>(src + t0, ids + t0, len, 0, per, cur2 + (size_t)S * per, offsets + (size_t)S * per,
@@ -849,7 +839,7 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
             item_s[0] = item_s[1];
             const int nb = (int)atomicAdd(counter, 1u);
             item_s[1] = nb;
-            if (nb < buckets) lm_prefetch_l2(in + offsets[nb], in + offsets[nb + 1]);
+            if (nb < buckets) prefetch_l2(in + offsets[nb], in + offsets[nb + 1]);
         }
         __syncthreads();
         const int b = item_s[0];

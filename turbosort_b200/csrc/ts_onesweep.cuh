@@ -121,7 +121,7 @@ __device__ __forceinline__ void st_relaxed_gpu_v4(uint32_t* p, const uint32_t (&
 // rest use PeerMasks. The split keeps both pipes busy.
 template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
           int MATCH_CNT>
-__global__ void __launch_bounds__(THREADS, 2) k_onesweep(SweepArgs<U, PAIRS> a) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<U, PAIRS> a) {
     using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
     using OFF = typename std::conditional<BIG, long long, int>::type;
     constexpr int RADIX = L::RADIX;
@@ -396,11 +396,27 @@ __global__ void __launch_bounds__(THREADS, 2) k_onesweep(SweepArgs<U, PAIRS> a) 
             __syncthreads();
         }
     } else {
+        // one buffer: each CTA holds the claim on its next tile while it works
+        // on this one, and brings that tile into L2 meanwhile, so the copy into
+        // shared memory that starts the next iteration reads from L2
+        if (tid == 0) misc[1] = (int)atomicAdd(a.tile_counter, 1u);
         for (;;) {
             if (tid == 0) {
-                const int t = (int)atomicAdd(a.tile_counter, 1u);
+                const int t = misc[1];
                 misc[0] = t;
-                if (t < a.portion_tiles) issue(t, 0);
+                if (t < a.portion_tiles) {
+                    issue(t, 0);
+                    const int nx = (int)atomicAdd(a.tile_counter, 1u);
+                    misc[1] = nx;
+                    if (nx < a.portion_tiles) {
+                        const size_t nb = a.portion_begin + (size_t)nx * TILE;
+                        const size_t ne = min(portion_end, nb + TILE);
+                        prefetch_l2(src + nb, src + ne);
+                        if constexpr (PAIRS) {
+                            if (!first) prefetch_l2(vsrc + nb, vsrc + ne);
+                        }
+                    }
+                }
             }
             __syncthreads();
             const int t = misc[0];
