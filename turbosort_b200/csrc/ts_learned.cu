@@ -222,11 +222,11 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     const int split_tiles = (int)((n + LM_SPLIT_TILE - 1) / LM_SPLIT_TILE);
     mark(c, "lm_split");
     cudaEventRecord(ev.e[4], c->stream);
-    const int split_grid = std::min(split_tiles, c->sm_count);
-    k_lm_split1<U><<<split_grid, 1024, LmSplitSmem<U>::bytes, c->stream>>>(d, ids, n, blog - 7, B.cur1, B.offsets,
-                                                                           grouped, ids1, c->d_error);
-    k_lm_split2<U><<<c->sm_count, 1024, LmSplitSmem<U>::bytes, c->stream>>>(grouped, ids1, buckets, B.offsets,
-                                                                           B.tiles_before, B.cur2, part, c->d_error);
+    const int split_grid = std::min(split_tiles, 2 * c->sm_count);
+    k_lm_split1<U><<<split_grid, LM_SPLIT_THREADS, LmSplitSmem<U>::bytes, c->stream>>>(
+        d, ids, n, blog - 7, B.cur1, B.offsets, grouped, ids1, c->d_error);
+    k_lm_split2<U><<<2 * c->sm_count, LM_SPLIT_THREADS, LmSplitSmem<U>::bytes, c->stream>>>(
+        grouped, ids1, buckets, B.offsets, B.tiles_before, B.cur2, part, c->d_error);
     c->launches += 2;
     mark(c, "lm_finish");
     cudaEventRecord(ev.e[5], c->stream);

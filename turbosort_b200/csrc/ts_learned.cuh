@@ -542,7 +542,8 @@ __global__ void __launch_bounds__(1024) k_lm_count(const U* __restrict__ src, si
 
 constexpr int LM_SUPERS = 128;        // first scatter sweep: 128 groups of consecutive buckets
 constexpr int LM_SPLIT_IPT = 8;
-constexpr int LM_SPLIT_TILE = 1024 * LM_SPLIT_IPT;
+constexpr int LM_SPLIT_THREADS = 512;  // two CTAs an SM: one's barriers and loads overlap the other's work
+constexpr int LM_SPLIT_TILE = LM_SPLIT_THREADS * LM_SPLIT_IPT;
 
 // Exclusive scan of the bucket sizes into offsets[0..B], the largest bucket,
 // the scatter cursors (cur2[b] = offsets[b], cur1[S] = offsets[S * B/128]),
@@ -646,7 +647,7 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
     int slot[LM_SPLIT_IPT];
 #pragma unroll
     for (int e = 0; e < LM_SPLIT_IPT; ++e) {
-        const int i = e * 1024 + tid;
+        const int i = e * LM_SPLIT_THREADS + tid;
         if (i < len) {
             k[e] = src[i];
             id[e] = ids[i];
@@ -678,7 +679,7 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
     }
 #pragma unroll
     for (int e = 0; e < LM_SPLIT_IPT; ++e) {
-        const int i = e * 1024 + tid;
+        const int i = e * LM_SPLIT_THREADS + tid;
         if (i < len) {
             const int p = (int)start[(id[e] >> shift) & (bins - 1)] + slot[e];
             sk[p] = k[e];
@@ -686,7 +687,7 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
         }
     }
     __syncthreads();
-    for (int i = tid; i < len; i += 1024) {
+    for (int i = tid; i < len; i += LM_SPLIT_THREADS) {
         const int d = (sid[i] >> shift) & (bins - 1);
         const unsigned long long g = gbase[d] + (unsigned long long)(i - (int)start[d]);
         if (g < gend[d]) {
@@ -703,7 +704,7 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
 // Persistent CTAs take every gridDim.x-th tile and prefetch the next one into
 // L2 while they work on the current one.
 template <typename U>
-__global__ void __launch_bounds__(1024, 1) k_lm_split1(const U* __restrict__ src, const unsigned short* __restrict__ ids,
+__global__ void __launch_bounds__(LM_SPLIT_THREADS, 2) k_lm_split1(const U* __restrict__ src, const unsigned short* __restrict__ ids,
                                                        size_t n, int shift, unsigned long long* __restrict__ cur1,
                                                        const unsigned long long* __restrict__ offsets,
                                                        U* __restrict__ dst, unsigned short* __restrict__ dst_ids,
@@ -743,7 +744,7 @@ __device__ __forceinline__ int lm_tile2(unsigned int tile, int per, const unsign
 // Second sweep: inside each group, keys to their buckets; persistent CTAs
 // with the next tile prefetched into L2, as in the first sweep.
 template <typename U>
-__global__ void __launch_bounds__(1024, 1) k_lm_split2(const U* __restrict__ src, const unsigned short* __restrict__ ids,
+__global__ void __launch_bounds__(LM_SPLIT_THREADS, 2) k_lm_split2(const U* __restrict__ src, const unsigned short* __restrict__ ids,
                                                        int buckets, const unsigned long long* __restrict__ offsets,
                                                        const unsigned int* __restrict__ tiles_before,
                                                        unsigned long long* __restrict__ cur2, U* __restrict__ dst,
@@ -771,14 +772,16 @@ __global__ void __launch_bounds__(1024, 1) k_lm_split2(const U* __restrict__ src
 // ---- bucket finish -----------------------------------------------------------
 // Every bucket sorted from `in` (the partition) into `out`, one CTA a bucket
 // at a time. A bucket that fits in shared memory takes one MSD digit pass:
-// its keys' range [kmin, kmax] is cut into up to 2048 equal sub-ranges (a
-// monotone map, so the sub-ranges are ordered), keys are counted and placed
-// by sub-range in shared memory, and each thread insertion-sorts its
-// sub-ranges (at most LM_SUB_MAX keys each). Buckets above the capacity, or
-// whose keys crowd one sub-range, take the CTA-level LSD through `scratch`.
-constexpr int LM_FIN_SMEM = 200 * 1024;
-constexpr int LM_SUB_BITS = 11;
-constexpr int LM_SUB_MAX = 64;
+// its keys' range [kmin, kmax] is cut into up to 2^14 equal sub-ranges (a
+// monotone map, so the sub-ranges are ordered; about one key each), keys are
+// counted and placed by sub-range in shared memory with 16-bit counters, and
+// each thread insertion-sorts the run of consecutive sub-ranges it owns (the
+// run is out of order only inside its sub-ranges, so this costs about one
+// step a key). Buckets above the capacity, or whose keys crowd one sub-range
+// (LM_SUB_MAX keys), take the CTA-level LSD through `scratch`.
+constexpr int LM_FIN_SMEM = 227 * 1024;
+constexpr int LM_SUB_BITS = 14;
+constexpr int LM_SUB_MAX = 128;
 
 // fn(i, src[i]) for this thread's share of 0..len-1, its loads issued a
 // group at a time (one bucket is read by one CTA: latency, not bandwidth,
@@ -803,10 +806,9 @@ __device__ __forceinline__ void lm_for_keys(const U* __restrict__ src, int len, 
 
 template <typename U>
 struct LmFinSmem {
-    static constexpr size_t misc = LM_FIN_SMEM - 1024;                       // warp totals, reductions
-    static constexpr size_t start = misc - (size_t)((1 << LM_SUB_BITS) + 32) * 4;
-    static constexpr size_t hist = start - (size_t)(1 << LM_SUB_BITS) * 4;
-    static constexpr int cap = (int)(hist / sizeof(U));                      // keys sorted by the MSD pass
+    static constexpr size_t misc = LM_FIN_SMEM - 1024;                    // warp totals, reductions
+    static constexpr size_t words = misc - (size_t)(1 << LM_SUB_BITS) * 2;  // 16-bit counters, two a word
+    static constexpr int cap = (int)(words / sizeof(U)) < 65535 ? (int)(words / sizeof(U)) : 65535;
 };
 
 template <typename U, int XF>
@@ -817,10 +819,9 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
     extern __shared__ __align__(16) unsigned char fsm[];
     using F = LmFinSmem<U>;
     U* sk = reinterpret_cast<U*>(fsm);
-    unsigned int* hist = reinterpret_cast<unsigned int*>(fsm + F::hist);
-    unsigned int* start = reinterpret_cast<unsigned int*>(fsm + F::start);
+    unsigned int* wd = reinterpret_cast<unsigned int*>(fsm + F::words);  // counter d: half (d & 1) of wd[d >> 1]
     int* misc = reinterpret_cast<int*>(fsm + F::misc);
-    int* warp_tot = misc;                                                 // [32]
+    int* warp_tot = misc;                                                         // [32]
     unsigned long long* red = reinterpret_cast<unsigned long long*>(misc + 32);  // [4]
     int* item_s = misc + 40;
     // the CTA-level LSD's areas, inside the key area (unused while it runs)
@@ -828,6 +829,7 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
     uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
     uint32_t* l_run = l_hist + 8 * 256;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    auto half = [](unsigned int w, int d) { return (w >> ((d & 1) * 16)) & 0xffffu; };
     if (tid == 0) {
         red[2] = 0ull;
         item_s[1] = (int)atomicAdd(counter, 1u);
@@ -855,7 +857,7 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
         }
         bool large = len > F::cap;
         unsigned long long kmin = 0, kmax = 0;
-        int bits = 0;
+        int bits = 1;
         if (!large) {
             // pass 1: the bucket's key range
             if (tid == 0) {
@@ -870,10 +872,10 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
                 mx = k > mx ? k : mx;
             });
             for (int o = 16; o > 0; o >>= 1) {
-                const unsigned long long a = __shfl_xor_sync(0xffffffffu, mn, o);
-                const unsigned long long c = __shfl_xor_sync(0xffffffffu, mx, o);
-                mn = a < mn ? a : mn;
-                mx = c > mx ? c : mx;
+                const unsigned long long x = __shfl_xor_sync(0xffffffffu, mn, o);
+                const unsigned long long y = __shfl_xor_sync(0xffffffffu, mx, o);
+                mn = x < mn ? x : mn;
+                mx = y > mx ? y : mx;
             }
             if (lane == 0) {
                 atomicMin(&red[0], mn);
@@ -887,35 +889,48 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
                 __syncthreads();
                 continue;
             }
-            bits = 1;
-            while (bits < LM_SUB_BITS && (2 << bits) * 2 <= len) ++bits;  // about 2-4 keys a sub-range
+            while (bits < LM_SUB_BITS && (2 << bits) <= len) ++bits;  // about one or two keys a sub-range
         }
         const int nb = 1 << bits;
+        const int per = nb >= 2048 ? nb / 1024 : 2;  // counters a thread scans and sorts (even)
+        const int owners = nb / per;
         const float scale = large ? 0.f : (float)nb / __ull2float_ru(kmax - kmin);
         auto digit = [&](unsigned long long k) { return min(nb - 1, (int)(__ull2float_rz(k - kmin) * scale)); };
         if (!large) {
-            // pass 2: counts per sub-range, their starts, the largest
-            for (int d = tid; d < nb; d += 1024) hist[d] = 0;
+            // pass 2: counts per sub-range
+            for (int w = tid; w < nb / 2; w += 1024) wd[w] = 0u;
             __syncthreads();
-            lm_for_keys<U>(src, len,
-                           [&](int, U v) { atomicAdd(&hist[digit((unsigned long long)to_key<U, XF>(v))], 1u); });
+            lm_for_keys<U>(src, len, [&](int, U v) {
+                const int d = digit((unsigned long long)to_key<U, XF>(v));
+                atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16));
+            });
             __syncthreads();
-            unsigned int v0 = 2 * tid < nb ? hist[2 * tid] : 0u, v1 = 2 * tid + 1 < nb ? hist[2 * tid + 1] : 0u;
-            unsigned int x = v0 + v1, m = max(v0, v1);
+            // exclusive scan of the counters (each owner a run of `per`), their largest
+            unsigned int sum = 0, m = 0;
+            if (tid < owners)
+                for (int q = 0; q < per / 2; ++q) {
+                    const unsigned int w = wd[tid * (per / 2) + q];
+                    sum += (w & 0xffffu) + (w >> 16);
+                    m = max(m, max(w & 0xffffu, w >> 16));
+                }
+            unsigned int x = sum;
             for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int yy = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += yy;
+                const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
             }
             for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
             if (lane == 31) warp_tot[warp] = (int)x;
             if (lane == 0) atomicMax(reinterpret_cast<unsigned int*>(&red[2]), m);
             __syncthreads();
-            unsigned int before = 0;
-            for (int w = 0; w < warp; ++w) before += (unsigned int)warp_tot[w];
-            const unsigned int s0 = before + x - v0 - v1;
-            if (2 * tid < nb) start[2 * tid] = s0;
-            if (2 * tid + 1 < nb) start[2 * tid + 1] = s0 + v0;
-            if (tid == 0) start[nb] = (unsigned int)len;
+            unsigned int run = x - sum;
+            for (int w = 0; w < warp; ++w) run += (unsigned int)warp_tot[w];
+            if (tid < owners)
+                for (int q = 0; q < per / 2; ++q) {
+                    const unsigned int w = wd[tid * (per / 2) + q];
+                    const unsigned int s0 = run, s1 = run + (w & 0xffffu);
+                    run = s1 + (w >> 16);
+                    wd[tid * (per / 2) + q] = s0 | (s1 << 16);  // starts, which become cursors
+                }
             __syncthreads();
             large = reinterpret_cast<unsigned int*>(&red[2])[0] > (unsigned int)LM_SUB_MAX;
             __syncthreads();
@@ -927,25 +942,26 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
             __syncthreads();
             continue;
         }
-        // pass 3: place keys by sub-range (cursor = hist, reset to the starts)
-        for (int d = tid; d < nb; d += 1024) hist[d] = start[d];
-        __syncthreads();
+        // pass 3: place keys by sub-range; each counter ends at its sub-range's end
         lm_for_keys<U>(src, len, [&](int, U v) {
             const U k = to_key<U, XF>(v);
-            sk[atomicAdd(&hist[digit((unsigned long long)k)], 1u)] = k;
+            const int d = digit((unsigned long long)k);
+            sk[half(atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16)), d)] = k;
         });
         __syncthreads();
-        // pass 4: every sub-range sorted by one thread
-        for (int d = tid; d < nb; d += 1024) {
-            const int s0 = (int)start[d], s1 = (int)start[d + 1];
-            for (int x = s0 + 1; x < s1; ++x) {
-                const U v = sk[x];
-                int y = x - 1;
-                while (y >= s0 && sk[y] > v) {
-                    sk[y + 1] = sk[y];
-                    --y;
+        // pass 4: every owner insertion-sorts its run of sub-ranges
+        if (tid < owners) {
+            const int d0 = tid * per;
+            const int r0 = d0 == 0 ? 0 : (int)half(wd[(d0 - 1) >> 1], d0 - 1);
+            const int r1 = (int)half(wd[(d0 + per - 1) >> 1], d0 + per - 1);
+            for (int i = r0 + 1; i < r1; ++i) {
+                const U v = sk[i];
+                int j = i - 1;
+                while (j >= r0 && sk[j] > v) {
+                    sk[j + 1] = sk[j];
+                    --j;
                 }
-                sk[y + 1] = v;
+                sk[j + 1] = v;
             }
         }
         __syncthreads();
