@@ -60,7 +60,7 @@ constexpr uint32_t LB_FLAG_AGG = 1u << 30;   // look-back: tile count only
 constexpr uint32_t LB_FLAG_INC = 2u << 30;   // look-back: inclusive prefix
 constexpr uint32_t LB_VALUE = (1u << 30) - 1;
 constexpr uint32_t SPIN_LIMIT = 1u << 20;    // bounded waits (about a second), then TS_ERR_TIMEOUT
-constexpr int LB_WINDOW = 8;                 // look-back entries loaded per round trip
+constexpr int LB_WINDOW = 4;                 // look-back entries loaded per round trip (4 beat 8, 16, 32 on a B200)
 constexpr uint32_t ERR_TIMEOUT = 1u;
 constexpr uint32_t ERR_BOUNDS = 2u;
 
