@@ -250,3 +250,33 @@ def test_large_u32_properties(ts):
     assert np.array_equal(np.bincount(a >> 20, minlength=4096), np.bincount(s >> 20, minlength=4096))
     assert int(a.astype(np.uint64).sum()) == int(s.astype(np.uint64).sum())
     assert np.array_equal(np.sort(a), s)
+
+
+@pytest.mark.parametrize("t", ["u32", "f32", "i64", "u16"])
+def test_repeated_sorts_of_one_buffer(ts, t):
+    """Repeated device sorts of the same buffer and size replay a captured
+    launch sequence (CUDA graph) from the third call on: every call must
+    still sort its new contents exactly, including presorted, reversed and
+    constant inputs whose plans differ from the captured call's."""
+    import torch
+
+    ctx = ts.Context(0)
+    rng = np.random.default_rng(23)
+    n = (1 << 18) + 7
+    d = None
+    launches = []
+    for shape in ["random", "random", "random", "desc", "asc", "const", "range16", "random"]:
+        a = gen(t, n, shape, rng)
+        if d is None:
+            d = to_dev(a, t)
+        else:
+            d.copy_(to_dev(a, t))
+        torch.cuda.synchronize()  # the copy ran on torch's stream, the sort runs on the context's
+        before = ts.lib().ts_ctx_launches(ctx.handle)
+        ts.sort(d, ctx)
+        ctx.synchronize()
+        launches.append(ts.lib().ts_ctx_launches(ctx.handle) - before)
+        assert from_dev(d, a).tobytes() == O.sort(a).tobytes(), (t, shape)
+    assert len(set(launches)) == 1, launches  # a replay counts the launches it holds
+    ctx.close()
+    torch.cuda.synchronize()

@@ -233,6 +233,7 @@ void ts_ctx_destroy(ts_ctx* c) {
     for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg, &c->learn})
         if (b->p) cudaFree(b->p);
     if (c->seg_graph) cudaGraphExecDestroy(c->seg_graph);
+    if (c->sort_graph) cudaGraphExecDestroy(c->sort_graph);
     if (c->d_error) cudaFree(c->d_error);
     for (auto& m : c->marks) cudaEventDestroy(m.second);
     for (auto ev : c->spare_events) cudaEventDestroy(ev);

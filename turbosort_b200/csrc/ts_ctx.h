@@ -46,6 +46,12 @@ struct ts_ctx {
     bool capturing = false;
     cudaGraphExec_t seg_graph = nullptr;
     size_t seg_graph_key[10] = {};
+    // plain device sort: the launch sequence of a repeated call, captured on
+    // its second identical call and replayed afterwards
+    cudaGraphExec_t sort_graph = nullptr;
+    size_t sort_graph_key[8] = {};
+    size_t sort_last_key[8] = {};
+    unsigned long long sort_graph_launches = 0;
 
     std::string last_error;
     unsigned long long launches = 0;   // kernels this context has launched

@@ -65,6 +65,7 @@ ts_status setup(int device, ts_ctx** out) {
         return TS_ERR_CUDA;
     }
     c->own_stream = false;
+    c->use_graphs = false;  // instantiating a graph could allocate
     c->alt.p = base;
     c->alt.cap = kAltBytes;
     c->lookback.p = base + kAltBytes;
