@@ -237,6 +237,24 @@ def workload_config(name: str, lg: int | None = None) -> dict:
             "parallelism": "replicas"}
 
 
+def reduce_over_ranks(torch, dist_mod, ms: float, ok: bool, device: str) -> tuple[float, bool]:
+    """The job's time is the slowest rank's (replicas start together after a
+    barrier); the job is correct only if every rank's output checked out.
+    Without a process group this rank is the job."""
+    if dist_mod is None:
+        return ms, ok
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+    okt = torch.tensor([0 if ok else 1], dtype=torch.int32, device=device)
+    dist_mod.all_reduce(okt, op=dist_mod.ReduceOp.MAX)
+    return float(t.item()), int(okt.item()) == 0
+
+
+def whole_job_gkeys(world: int, n_per_rank: int, ms_per_step: float) -> float:
+    """Keys sorted by all ranks per second (each rank sorts its own n keys a step)."""
+    return world * n_per_rank / (ms_per_step / 1e3) / 1e9
+
+
 def bench_device(ts, torch, ctx, kind, dist, lg, steps, warmup, seed, dist_mod, rank, world, timing=True):
     n = 1 << lg
     w = WIDTH[kind]
@@ -559,17 +577,10 @@ def main() -> None:
     r = bench_device(ts, torch, ctx, kind, dist, lg, args.steps, args.warmup, 0x9E3779B97F4A7C15 + rank, dist_mod,
                      rank, world)
     clk = clocks.stop()
-    ms = r["ms_total"]
-    if dist_mod is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
-        ms = float(t.item())
-        okt = torch.tensor([0 if r["ok"] else 1], device=f"cuda:{local}")
-        dist_mod.all_reduce(okt, op=dist_mod.ReduceOp.MAX)
-        r["ok"] = okt.item() == 0
+    ms, r["ok"] = reduce_over_ranks(torch, dist_mod, r["ms_total"], r["ok"], f"cuda:{local}")
     n, w, live = r["n"], r["w"], r["live"]
     ms_step = ms / args.steps
-    value = world * n / (ms_step / 1e3) / 1e9
+    value = whole_job_gkeys(world, n, ms_step)
 
     peak, peak_kind = measured_peak_gbs()
     sweep_ms, sweep_count = r["timings"].get("onesweep", (0.0, 0))
