@@ -466,7 +466,7 @@ def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True):
     return res
 
 
-def bench_learned(ts, torch, ctx, kind, steps, warmup, peak, lg=28):
+def bench_learned(ts, torch, ctx, kind, steps, warmup, peak, lg=28, buckets_log2=14):
     """Config 5: the learned-partition sort against the plain device LSD on the
     same 2^lg keys: f64 lognormal(0, 2), u64 from 8 Gaussians (means in
     [0, 2^60], sigma 2^40), f32 uniform [0, 1) with 10% duplicates. Model: 1024
@@ -484,7 +484,7 @@ def bench_learned(ts, torch, ctx, kind, steps, warmup, peak, lg=28):
     master = torch.from_numpy(host.view(np.int64 if w == 8 else np.int32)).to(dev)
     del host
     d = torch.empty_like(master)
-    p = ts.learned_params()
+    p = ts.learned_params(buckets_log2=buckets_log2)
 
     def timed(fn):
         tot = 0.0
@@ -543,11 +543,25 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--log2n", type=int, default=None, help="override the workload's size (profiling runs)")
+    ap.add_argument("--learned", default=None, choices=["lognormal_f64", "gauss_mix_u64", "unit_f32_dups"],
+                    help="only the learned-partition comparison on this input (2^log2n keys, default 2^28)")
+    ap.add_argument("--buckets-log2", type=int, default=14, help="buckets of the learned partition (with --learned)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.learned:
+        import torch
+
+        import turbosort_b200 as ts
+
+        ctx = ts.Context(0)
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        res = bench_learned(ts, torch, ctx, args.learned, args.steps, args.warmup, measured_peak_gbs()[0],
+                            lg=args.log2n or 28, buckets_log2=args.buckets_log2)
+        print(json.dumps({"learned": args.learned, **res}), flush=True)
         return
 
     import torch

@@ -608,31 +608,40 @@ __global__ void __launch_bounds__(1024) k_lm_bucket_scan(const unsigned long lon
     }
 }
 
-// Shared memory of a scatter sweep: keys, bucket ids, per-digit counts,
-// starts and reserved global bases.
+// Shared memory of a scatter sweep: the staged tile as it arrives (keys and
+// bucket ids, each with 32 bytes of room: a copy widened to 16-byte bounds
+// at both ends adds at most 15 + 15 bytes), the tile grouped by digit,
+// per-digit counts, starts, reserved global bases and range ends, and the
+// staging barrier.
 template <typename U>
 struct LmSplitSmem {
-    static constexpr size_t keys = 0;
-    static constexpr size_t ids = (size_t)LM_SPLIT_TILE * sizeof(U);
-    static constexpr size_t cnt = ids + (size_t)LM_SPLIT_TILE * 2;
+    static constexpr size_t al(size_t x) { return (x + 15) / 16 * 16; }
+    static constexpr size_t stage_k = 0;
+    static constexpr size_t stage_i = al(stage_k + (size_t)LM_SPLIT_TILE * sizeof(U) + 32);
+    static constexpr size_t keys = al(stage_i + (size_t)LM_SPLIT_TILE * 2 + 32);
+    static constexpr size_t ids = keys + (size_t)LM_SPLIT_TILE * sizeof(U);
+    static constexpr size_t cnt = al(ids + (size_t)LM_SPLIT_TILE * 2);
     static constexpr size_t start = cnt + 256 * 4;
     static constexpr size_t gbase = start + 256 * 4;
     static constexpr size_t gend = gbase + 256 * 8;
-    static constexpr size_t bytes = gend + 256 * 8 + 64;
+    static constexpr size_t bar = gend + 256 * 8;
+    static constexpr size_t bytes = bar + 64;
 };
 
-// One scatter tile: `len` keys and ids from src, grouped in shared memory by
+// One scatter tile: `len` keys and ids (staged in shared memory), grouped by
 // digit = (id >> shift) & (bins - 1), each digit's run written at a range of
 // dst reserved with one atomic on cur[digit] (the order inside a bucket is
 // free: the buckets are sorted afterwards), so the stores are coalesced runs.
 // Digit d's range of dst ends at ends[(d + 1) * end_stride]; a store past it
-// (counts that disagree with the ids) is dropped and flagged.
-template <typename U, bool WRITE_IDS>
-__device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const unsigned short* __restrict__ ids, int len,
-                                              int shift, int bins, unsigned long long* __restrict__ cur,
+// (counts that disagree with the ids) is dropped and flagged. `staged` runs
+// (on every thread) once the staging area has been read, so the next tile
+// can start arriving there.
+template <typename U, bool WRITE_IDS, typename Staged>
+__device__ __forceinline__ void lm_split_tile(const U* src, const unsigned short* ids, int len, int shift, int bins,
+                                              unsigned long long* __restrict__ cur,
                                               const unsigned long long* __restrict__ ends, int end_stride,
                                               U* __restrict__ dst, unsigned short* __restrict__ dst_ids,
-                                              unsigned char* sm, uint32_t* __restrict__ error) {
+                                              unsigned char* sm, uint32_t* __restrict__ error, Staged staged) {
     U* sk = reinterpret_cast<U*>(sm + LmSplitSmem<U>::keys);
     unsigned short* sid = reinterpret_cast<unsigned short*>(sm + LmSplitSmem<U>::ids);
     unsigned int* cnt = reinterpret_cast<unsigned int*>(sm + LmSplitSmem<U>::cnt);
@@ -655,6 +664,7 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
         }
     }
     __syncthreads();
+    staged();
     if (warp < 8) {  // exclusive scan of cnt[0..256), one warp a 32-digit slice, then across slices
         const int d = warp * 32 + lane;
         const unsigned int v = d < bins ? cnt[d] : 0u;
@@ -700,27 +710,82 @@ __device__ __forceinline__ void lm_split_tile(const U* __restrict__ src, const u
     __syncthreads();
 }
 
+// A persistent sweep's staging: bulk copies (no multicast) of a tile's keys
+// and ids into shared memory, completing on one mbarrier. A tile that starts
+// off a 16-byte boundary is copied from the boundary below (and up to the
+// boundary above its end: neither crosses a page), and read from `pre`
+// elements in.
+template <typename U>
+struct LmStage {
+    unsigned char* sm;
+    uint64_t* bar;
+    uint32_t parity;
+    __device__ static int pre_k(const U* p) { return (int)(((uintptr_t)p & 15) / sizeof(U)); }
+    __device__ static int pre_i(const unsigned short* p) { return (int)(((uintptr_t)p & 15) / 2); }
+    // thread 0: start the copy of [k, k + len) and [i, i + len)
+    __device__ void issue(const U* k, const unsigned short* i, int len) {
+        if (len <= 0) {
+            mbar_arrive_expect_tx(bar, 0);
+            return;
+        }
+        const uintptr_t ka = (uintptr_t)k & ~(uintptr_t)15, kz = ((uintptr_t)(k + len) + 15) & ~(uintptr_t)15;
+        const uintptr_t ia = (uintptr_t)i & ~(uintptr_t)15, iz = ((uintptr_t)(i + len) + 15) & ~(uintptr_t)15;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(bar, (uint32_t)((kz - ka) + (iz - ia)));
+        bulk_g2s(sm + LmSplitSmem<U>::stage_k, (const void*)ka, (uint32_t)(kz - ka), bar);
+        bulk_g2s(sm + LmSplitSmem<U>::stage_i, (const void*)ia, (uint32_t)(iz - ia), bar);
+    }
+    // every thread: wait for the copy (bounded; a timeout is flagged and the
+    // tile's writes stay inside their ranges)
+    __device__ void wait(uint32_t* error) {
+        if (!mbar_wait(bar, parity)) atomicOr(error, ERR_TIMEOUT);
+        parity ^= 1u;
+    }
+};
+
 // First sweep: keys (and ids) into LM_SUPERS groups of consecutive buckets.
-// Persistent CTAs take every gridDim.x-th tile and prefetch the next one into
-// L2 while they work on the current one.
+// Persistent CTAs take every gridDim.x-th tile; the next tile's copy into
+// shared memory starts as soon as this tile's keys are in registers.
 template <typename U>
 __global__ void __launch_bounds__(LM_SPLIT_THREADS, 2) k_lm_split1(const U* __restrict__ src, const unsigned short* __restrict__ ids,
                                                        size_t n, int shift, unsigned long long* __restrict__ cur1,
                                                        const unsigned long long* __restrict__ offsets,
                                                        U* __restrict__ dst, unsigned short* __restrict__ dst_ids,
                                                        uint32_t* __restrict__ error) {
-    extern __shared__ __align__(16) unsigned char ssm[];
+    extern __shared__ __align__(128) unsigned char ssm[];
     const size_t tiles = (n + LM_SPLIT_TILE - 1) / LM_SPLIT_TILE;
-    for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const size_t t0 = tile * LM_SPLIT_TILE;
-        const int len = (int)min((size_t)LM_SPLIT_TILE, n - t0);
-        if (threadIdx.x == 0 && tile + gridDim.x < tiles) {
-            const size_t u0 = t0 + (size_t)gridDim.x * LM_SPLIT_TILE, u1 = min(n, u0 + LM_SPLIT_TILE);
-            prefetch_l2(src + u0, src + u1);
-            prefetch_l2(ids + u0, ids + u1);
+    LmStage<U> st{ssm, reinterpret_cast<uint64_t*>(ssm + LmSplitSmem<U>::bar), 0u};
+    auto span = [&](size_t tile, size_t& t0, int& len) {
+        t0 = tile * LM_SPLIT_TILE;
+        len = (int)min((size_t)LM_SPLIT_TILE, n - t0);
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(st.bar, 1);
+        fence_mbar_init();
+        if (blockIdx.x < tiles) {
+            size_t t0;
+            int len;
+            span(blockIdx.x, t0, len);
+            st.issue(src + t0, ids + t0, len);
         }
-        lm_split_tile<U, true>(src + t0, ids + t0, len, shift, LM_SUPERS, cur1, offsets, 1 << shift, dst, dst_ids, ssm,
-                               error);
+    }
+    __syncthreads();
+    for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        size_t t0;
+        int len;
+        span(tile, t0, len);
+        st.wait(error);
+        const U* sk = reinterpret_cast<const U*>(ssm + LmSplitSmem<U>::stage_k) + LmStage<U>::pre_k(src + t0);
+        const unsigned short* si =
+            reinterpret_cast<const unsigned short*>(ssm + LmSplitSmem<U>::stage_i) + LmStage<U>::pre_i(ids + t0);
+        lm_split_tile<U, true>(sk, si, len, shift, LM_SUPERS, cur1, offsets, 1 << shift, dst, dst_ids, ssm, error, [&] {
+            if (threadIdx.x == 0 && tile + gridDim.x < tiles) {
+                size_t u0;
+                int ulen;
+                span(tile + gridDim.x, u0, ulen);
+                st.issue(src + u0, ids + u0, ulen);
+            }
+        });
     }
 }
 
@@ -742,30 +807,45 @@ __device__ __forceinline__ int lm_tile2(unsigned int tile, int per, const unsign
 }
 
 // Second sweep: inside each group, keys to their buckets; persistent CTAs
-// with the next tile prefetched into L2, as in the first sweep.
+// with the next tile's copy started early, as in the first sweep.
 template <typename U>
 __global__ void __launch_bounds__(LM_SPLIT_THREADS, 2) k_lm_split2(const U* __restrict__ src, const unsigned short* __restrict__ ids,
                                                        int buckets, const unsigned long long* __restrict__ offsets,
                                                        const unsigned int* __restrict__ tiles_before,
                                                        unsigned long long* __restrict__ cur2, U* __restrict__ dst,
                                                        uint32_t* __restrict__ error) {
-    extern __shared__ __align__(16) unsigned char ssm[];
+    extern __shared__ __align__(128) unsigned char ssm[];
     const unsigned int tiles = tiles_before[LM_SUPERS];
     const int per = buckets / LM_SUPERS;
+    LmStage<U> st{ssm, reinterpret_cast<uint64_t*>(ssm + LmSplitSmem<U>::bar), 0u};
+    if (threadIdx.x == 0) {
+        mbar_init(st.bar, 1);
+        fence_mbar_init();
+        if (blockIdx.x < tiles) {
+            unsigned long long t0;
+            int len;
+            lm_tile2(blockIdx.x, per, offsets, tiles_before, t0, len);
+            st.issue(src + t0, ids + t0, len);
+        }
+    }
+    __syncthreads();
     for (unsigned int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         unsigned long long t0;
         int len;
         const int S = lm_tile2(tile, per, offsets, tiles_before, t0, len);
-        if (threadIdx.x == 0 && tile + gridDim.x < tiles) {
-            unsigned long long u0;
-            int ulen;
-            lm_tile2(tile + gridDim.x, per, offsets, tiles_before, u0, ulen);
-            prefetch_l2(src + u0, src + u0 + ulen);
-            prefetch_l2(ids + u0, ids + u0 + ulen);
-        }
-        if (len > 0)  // uniform over the CTA
-            lm_split_tile<U, false>(src + t0, ids + t0, len, 0, per, cur2 + (size_t)S * per, offsets + (size_t)S * per,
-                                    1, dst, nullptr, ssm, error);
+        st.wait(error);
+        const U* sk = reinterpret_cast<const U*>(ssm + LmSplitSmem<U>::stage_k) + LmStage<U>::pre_k(src + t0);
+        const unsigned short* si =
+            reinterpret_cast<const unsigned short*>(ssm + LmSplitSmem<U>::stage_i) + LmStage<U>::pre_i(ids + t0);
+        lm_split_tile<U, false>(sk, si, len, 0, per, cur2 + (size_t)S * per, offsets + (size_t)S * per, 1, dst, nullptr,
+                                ssm, error, [&] {
+                                    if (threadIdx.x == 0 && tile + gridDim.x < tiles) {
+                                        unsigned long long u0;
+                                        int ulen;
+                                        lm_tile2(tile + gridDim.x, per, offsets, tiles_before, u0, ulen);
+                                        st.issue(src + u0, ids + u0, ulen);
+                                    }
+                                });
     }
 }
 
