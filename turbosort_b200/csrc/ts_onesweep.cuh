@@ -4,16 +4,17 @@
 // Per tile (THREADS x IPT keys), in a persistent CTA that takes tiles in
 // order from a counter:
 //   1. the keys arrive in shared memory by one bulk copy (cp.async.bulk, no
-//      multicast), issued one tile ahead so the next tile streams in while
-//      this one is ranked;
+//      multicast); with two buffers (NBUF = 2) it is issued one tile ahead,
+//      with one the CTA claims its next tile early and prefetches it into L2;
 //   2. a counting pass builds per-warp digit counts, the tile's
 //      digit counts are published to the look-back array at once, and the
 //      tile-local start of every (digit, warp) run is scanned;
-//   3. a ranking pass finds each key's equals inside its warp with one ballot
-//      per digit bit and writes the key straight to its sorted place in a
-//      shared staging tile (stable: warp order, then item order, then lane);
+//   3. a ranking pass finds each key's equals inside its warp (one ballot per
+//      digit bit, or match.any for some items) and writes the key straight to
+//      its sorted place in a shared staging tile (stable: warp order, then
+//      item order, then lane);
 //   4. the digit owners finish the look-back (keys of their digit in all
-//      earlier tiles) while no other work waits on it;
+//      earlier tiles), a few predecessors per round trip;
 //   5. the staged tile goes out as runs per digit: consecutive threads write
 //      consecutive addresses.
 // The key transform (src/key.rs:135-197) is applied as the first pass reads
@@ -103,18 +104,6 @@ struct PeerMasks {
         return p;
     }
 };
-
-__device__ __forceinline__ void ld_relaxed_gpu_v4(const uint32_t* p, uint32_t (&v)[4]) {
-    asm volatile("ld.relaxed.gpu.global.v4.u32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
-                 : "l"(p)
-                 : "memory");
-}
-__device__ __forceinline__ void st_relaxed_gpu_v4(uint32_t* p, const uint32_t (&v)[4]) {
-    asm volatile("st.relaxed.gpu.global.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(v[0]), "r"(v[1]), "r"(v[2]),
-                 "r"(v[3])
-                 : "memory");
-}
 
 // Items i with i % MATCH_MOD < MATCH_CNT find their equal digits with the
 // match.any instruction, which runs on a different pipe from the ballots; the
