@@ -132,7 +132,7 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     TS_CUDA(c, cudaFuncSetAttribute((const void*)k_lm_split2<U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)LmSplitSmem<U>::bytes));
     TS_CUDA(c, cudaFuncSetAttribute((const void*)k_lm_finish<U, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    LM_FIN_SMEM));
+                                    MSD_SMEM));
 
     Events ev;
     mark(c, "lm_sample");
@@ -230,7 +230,7 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     c->launches += 2;
     mark(c, "lm_finish");
     cudaEventRecord(ev.e[5], c->stream);
-    k_lm_finish<U, XF><<<c->sm_count, 1024, LM_FIN_SMEM, c->stream>>>(part, d, grouped, B.offsets, buckets, B.counter);
+    k_lm_finish<U, XF><<<c->sm_count, 1024, MSD_SMEM, c->stream>>>(part, d, grouped, B.offsets, buckets, B.counter);
     ++c->launches;
     TS_CUDA(c, cudaGetLastError());
     cudaEventRecord(ev.e[6], c->stream);

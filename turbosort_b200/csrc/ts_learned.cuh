@@ -851,72 +851,20 @@ __global__ void __launch_bounds__(LM_SPLIT_THREADS, 2) k_lm_split2(const U* __re
 
 // ---- bucket finish -----------------------------------------------------------
 // Every bucket sorted from `in` (the partition) into `out`, one CTA a bucket
-// at a time. A bucket that fits in shared memory takes one MSD digit pass:
-// its keys' range [kmin, kmax] is cut into up to 2^14 equal sub-ranges (a
-// monotone map, so the sub-ranges are ordered; about one key each), keys are
-// counted and placed by sub-range in shared memory with 16-bit counters, and
-// each thread insertion-sorts the run of consecutive sub-ranges it owns (the
-// run is out of order only inside its sub-ranges, so this costs about one
-// step a key). Buckets above the capacity, or whose keys crowd one sub-range
-// (LM_SUB_MAX keys), take the CTA-level LSD through `scratch`.
-constexpr int LM_FIN_SMEM = 227 * 1024;
-constexpr int LM_SUB_BITS = 14;
-constexpr int LM_SUB_MAX = 128;
-
-// fn(i, src[i]) for this thread's share of 0..len-1, its loads issued a
-// group at a time (one bucket is read by one CTA: latency, not bandwidth,
-// bounds a plain loop)
-template <typename U, typename Fn>
-__device__ __forceinline__ void lm_for_keys(const U* __restrict__ src, int len, Fn fn) {
-    constexpr int G = 32 / sizeof(U);
-    for (int base = threadIdx.x; base < len; base += 1024 * G) {
-        U v[G];
-#pragma unroll
-        for (int e = 0; e < G; ++e) {
-            const int i = base + e * 1024;
-            v[e] = i < len ? src[i] : (U)0;
-        }
-#pragma unroll
-        for (int e = 0; e < G; ++e) {
-            const int i = base + e * 1024;
-            if (i < len) fn(i, v[e]);
-        }
-    }
-}
-
-template <typename U>
-struct LmFinSmem {
-    static constexpr size_t misc = LM_FIN_SMEM - 1024;                    // warp totals, reductions
-    static constexpr size_t words = misc - (size_t)(1 << LM_SUB_BITS) * 2;  // 16-bit counters, two a word
-    static constexpr int cap = (int)(words / sizeof(U)) < 65535 ? (int)(words / sizeof(U)) : 65535;
-};
-
+// at a time, by the segmented sort's MSD routine (msd_sort: one digit pass
+// over the bucket's key range in shared memory, the CTA-level LSD for
+// buckets above its capacity). The next bucket is claimed early and brought
+// into L2 while this one is sorted.
 template <typename U, int XF>
 __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in, U* __restrict__ out,
                                                        U* __restrict__ scratch,
                                                        const unsigned long long* __restrict__ offsets, int buckets,
                                                        unsigned int* __restrict__ counter) {
     extern __shared__ __align__(16) unsigned char fsm[];
-    using F = LmFinSmem<U>;
-    U* sk = reinterpret_cast<U*>(fsm);
-    unsigned int* wd = reinterpret_cast<unsigned int*>(fsm + F::words);  // counter d: half (d & 1) of wd[d >> 1]
-    int* misc = reinterpret_cast<int*>(fsm + F::misc);
-    int* warp_tot = misc;                                                         // [32]
-    unsigned long long* red = reinterpret_cast<unsigned long long*>(misc + 32);  // [4]
-    int* item_s = misc + 40;
-    // the CTA-level LSD's areas, inside the key area (unused while it runs)
-    uint32_t* l_cnt = reinterpret_cast<uint32_t*>(fsm + (size_t)SegCfg<U>::LARGE_TILE * sizeof(U));
-    uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
-    uint32_t* l_run = l_hist + 8 * 256;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    auto half = [](unsigned int w, int d) { return (w >> ((d & 1) * 16)) & 0xffffu; };
-    if (tid == 0) {
-        red[2] = 0ull;
-        item_s[1] = (int)atomicAdd(counter, 1u);
-    }
+    int* item_s = reinterpret_cast<int*>(fsm + MsdSmem<U>::misc) + 48;
+    const int tid = threadIdx.x;
+    if (tid == 0) item_s[1] = (int)atomicAdd(counter, 1u);
     for (;;) {
-        // take the bucket claimed last time, claim the next one and start
-        // bringing it into L2 while this one is sorted
         if (tid == 0) {
             item_s[0] = item_s[1];
             const int nb = (int)atomicAdd(counter, 1u);
@@ -928,125 +876,7 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
         __syncthreads();
         if (b >= buckets) break;
         const unsigned long long lo = offsets[b];
-        const int len = (int)(offsets[b + 1] - lo);
-        const U* src = in + lo;
-        U* dst = out + lo;
-        if (len <= 1) {
-            if (len == 1 && tid == 0) dst[0] = src[0];
-            continue;
-        }
-        bool large = len > F::cap;
-        unsigned long long kmin = 0, kmax = 0;
-        int bits = 1;
-        if (!large) {
-            // pass 1: the bucket's key range
-            if (tid == 0) {
-                red[0] = ~0ull;
-                red[1] = 0ull;
-            }
-            __syncthreads();
-            unsigned long long mn = ~0ull, mx = 0ull;
-            lm_for_keys<U>(src, len, [&](int, U v) {
-                const unsigned long long k = (unsigned long long)to_key<U, XF>(v);
-                mn = k < mn ? k : mn;
-                mx = k > mx ? k : mx;
-            });
-            for (int o = 16; o > 0; o >>= 1) {
-                const unsigned long long x = __shfl_xor_sync(0xffffffffu, mn, o);
-                const unsigned long long y = __shfl_xor_sync(0xffffffffu, mx, o);
-                mn = x < mn ? x : mn;
-                mx = y > mx ? y : mx;
-            }
-            if (lane == 0) {
-                atomicMin(&red[0], mn);
-                atomicMax(&red[1], mx);
-            }
-            __syncthreads();
-            kmin = red[0];
-            kmax = red[1];
-            if (kmin == kmax) {  // every key equal
-                lm_for_keys<U>(src, len, [&](int i, U v) { dst[i] = v; });
-                __syncthreads();
-                continue;
-            }
-            while (bits < LM_SUB_BITS && (2 << bits) <= len) ++bits;  // about one or two keys a sub-range
-        }
-        const int nb = 1 << bits;
-        const int per = nb >= 2048 ? nb / 1024 : 2;  // counters a thread scans and sorts (even)
-        const int owners = nb / per;
-        const float scale = large ? 0.f : (float)nb / __ull2float_ru(kmax - kmin);
-        auto digit = [&](unsigned long long k) { return min(nb - 1, (int)(__ull2float_rz(k - kmin) * scale)); };
-        if (!large) {
-            // pass 2: counts per sub-range
-            for (int w = tid; w < nb / 2; w += 1024) wd[w] = 0u;
-            __syncthreads();
-            lm_for_keys<U>(src, len, [&](int, U v) {
-                const int d = digit((unsigned long long)to_key<U, XF>(v));
-                atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16));
-            });
-            __syncthreads();
-            // exclusive scan of the counters (each owner a run of `per`), their largest
-            unsigned int sum = 0, m = 0;
-            if (tid < owners)
-                for (int q = 0; q < per / 2; ++q) {
-                    const unsigned int w = wd[tid * (per / 2) + q];
-                    sum += (w & 0xffffu) + (w >> 16);
-                    m = max(m, max(w & 0xffffu, w >> 16));
-                }
-            unsigned int x = sum;
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-            if (lane == 31) warp_tot[warp] = (int)x;
-            if (lane == 0) atomicMax(reinterpret_cast<unsigned int*>(&red[2]), m);
-            __syncthreads();
-            unsigned int run = x - sum;
-            for (int w = 0; w < warp; ++w) run += (unsigned int)warp_tot[w];
-            if (tid < owners)
-                for (int q = 0; q < per / 2; ++q) {
-                    const unsigned int w = wd[tid * (per / 2) + q];
-                    const unsigned int s0 = run, s1 = run + (w & 0xffffu);
-                    run = s1 + (w >> 16);
-                    wd[tid * (per / 2) + q] = s0 | (s1 << 16);  // starts, which become cursors
-                }
-            __syncthreads();
-            large = reinterpret_cast<unsigned int*>(&red[2])[0] > (unsigned int)LM_SUB_MAX;
-            __syncthreads();
-            if (tid == 0) red[2] = 0ull;
-        }
-        if (large) {
-            seg_large_sort<U, XF>(src, dst, scratch + lo, len, sk, l_cnt, warp_tot, &red[3], l_hist, l_run, l_run + 256,
-                                  l_run + 512);
-            __syncthreads();
-            continue;
-        }
-        // pass 3: place keys by sub-range; each counter ends at its sub-range's end
-        lm_for_keys<U>(src, len, [&](int, U v) {
-            const U k = to_key<U, XF>(v);
-            const int d = digit((unsigned long long)k);
-            sk[half(atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16)), d)] = k;
-        });
-        __syncthreads();
-        // pass 4: every owner insertion-sorts its run of sub-ranges
-        if (tid < owners) {
-            const int d0 = tid * per;
-            const int r0 = d0 == 0 ? 0 : (int)half(wd[(d0 - 1) >> 1], d0 - 1);
-            const int r1 = (int)half(wd[(d0 + per - 1) >> 1], d0 + per - 1);
-            for (int i = r0 + 1; i < r1; ++i) {
-                const U v = sk[i];
-                int j = i - 1;
-                while (j >= r0 && sk[j] > v) {
-                    sk[j + 1] = sk[j];
-                    --j;
-                }
-                sk[j + 1] = v;
-            }
-        }
-        __syncthreads();
-        for (int i = tid; i < len; i += 1024) dst[i] = from_key<U, XF>(sk[i]);
-        __syncthreads();
+        msd_sort<U, XF>(in + lo, out + lo, scratch + lo, (int)(offsets[b + 1] - lo), fsm);
     }
 }
 

@@ -5,9 +5,11 @@
 // compare/src/main.rs:49-51); here a batch of slices given by offsets is
 // sorted at once. k_seg_bin puts each segment in a length bin; k_seg_sort is
 // one persistent launch whose CTAs take work items largest first:
-//   LARGE  one segment above the shared-memory capacity: a CTA-level LSD over
-//          its varying digits, tile by tile through a global scratch copy
-//          (the segment stays in L2), with running per-digit offsets;
+//   LARGE  one segment above the register capacity: one MSD digit pass over
+//          its key range in shared memory (msd_sort, 32- and 64-bit keys)
+//          while it fits there, else a CTA-level LSD over its varying digits, tile by tile
+//          through a global scratch copy (the segment stays in L2), with
+//          running per-digit offsets;
 //   BLOCK  one segment of up to CAP keys, sorted entirely on chip: keys in
 //          registers, one shared staging buffer, one stable pass per varying
 //          digit (radix with 4- or 8-bit digits) or a bitonic network, as the
@@ -345,6 +347,182 @@ __device__ void seg_large_sort(const U* in, U* seg, U* alt, int len, U* sm, uint
     }
 }
 
+// ---- MSD: one digit pass over a segment's key range, in shared memory -------
+// A segment of up to MsdSmem<U>::cap keys (24.8K of 8 bytes, 49.6K of 4) is
+// sorted with one MSD digit pass: its keys' range [kmin, kmax] is cut into up
+// to 2^14 equal sub-ranges (a monotone map, so the sub-ranges are ordered;
+// about one key each), keys are counted and placed by sub-range in shared
+// memory with 16-bit counters, and each thread insertion-sorts the run of
+// consecutive sub-ranges it owns (out of order only inside its sub-ranges).
+// Longer segments, or segments whose keys crowd one sub-range (MSD_SUB_MAX
+// keys), take the CTA-level LSD through `scratch`. src may equal dst.
+constexpr int MSD_SMEM = 227 * 1024;
+constexpr int MSD_SUB_BITS = 14;
+constexpr int MSD_SUB_MAX = 128;
+
+// fn(i, src[i]) for this thread's share of 0..len-1, its loads issued a
+// group at a time (one segment is read by one CTA: latency, not bandwidth,
+// bounds a plain loop)
+template <typename U, typename Fn>
+__device__ __forceinline__ void msd_for_keys(const U* __restrict__ src, int len, Fn fn) {
+    constexpr int G = 32 / sizeof(U);
+    for (int base = threadIdx.x; base < len; base += 1024 * G) {
+        U v[G];
+#pragma unroll
+        for (int e = 0; e < G; ++e) {
+            const int i = base + e * 1024;
+            v[e] = i < len ? src[i] : (U)0;
+        }
+#pragma unroll
+        for (int e = 0; e < G; ++e) {
+            const int i = base + e * 1024;
+            if (i < len) fn(i, v[e]);
+        }
+    }
+}
+
+template <typename U>
+struct MsdSmem {
+    static constexpr size_t misc = MSD_SMEM - 1024;                        // warp totals, reductions, item ids
+    static constexpr size_t words = misc - (size_t)(1 << MSD_SUB_BITS) * 2;  // 16-bit counters, two a word
+    static constexpr int cap = (int)(words / sizeof(U)) < 65535 ? (int)(words / sizeof(U)) : 65535;
+};
+
+// One segment, by the whole CTA (1024 threads); `sm` is MSD_SMEM bytes of
+// shared memory; `scratch` has room for len keys.
+template <typename U, int XF>
+__device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
+    using M = MsdSmem<U>;
+    U* sk = reinterpret_cast<U*>(sm);
+    unsigned int* wd = reinterpret_cast<unsigned int*>(sm + M::words);  // counter d: half (d & 1) of wd[d >> 1]
+    int* misc = reinterpret_cast<int*>(sm + M::misc);
+    int* warp_tot = misc;                                                         // [32]
+    unsigned long long* red = reinterpret_cast<unsigned long long*>(misc + 32);  // [4]
+    // the CTA-level LSD's areas, inside the key area (unused while it runs)
+    uint32_t* l_cnt = reinterpret_cast<uint32_t*>(sm + (size_t)SegCfg<U>::LARGE_TILE * sizeof(U));
+    uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
+    uint32_t* l_run = l_hist + 8 * 256;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    auto half = [](unsigned int w, int d) { return (w >> ((d & 1) * 16)) & 0xffffu; };
+    if (len <= 1) {
+        if (len == 1 && tid == 0) dst[0] = src[0];
+        return;
+    }
+    if (tid == 0) red[2] = 0ull;
+    bool large = len > M::cap;
+    unsigned long long kmin = 0, kmax = 0;
+    int bits = 1;
+    if (!large) {
+        // pass 1: the bucket's key range
+        if (tid == 0) {
+            red[0] = ~0ull;
+            red[1] = 0ull;
+        }
+        __syncthreads();
+        unsigned long long mn = ~0ull, mx = 0ull;
+        msd_for_keys<U>(src, len, [&](int, U v) {
+            const unsigned long long k = (unsigned long long)to_key<U, XF>(v);
+            mn = k < mn ? k : mn;
+            mx = k > mx ? k : mx;
+        });
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, mn, o);
+            const unsigned long long y = __shfl_xor_sync(0xffffffffu, mx, o);
+            mn = x < mn ? x : mn;
+            mx = y > mx ? y : mx;
+        }
+        if (lane == 0) {
+            atomicMin(&red[0], mn);
+            atomicMax(&red[1], mx);
+        }
+        __syncthreads();
+        kmin = red[0];
+        kmax = red[1];
+        if (kmin == kmax) {  // every key equal
+            msd_for_keys<U>(src, len, [&](int i, U v) { dst[i] = v; });
+            __syncthreads();
+            return;
+        }
+        while (bits < MSD_SUB_BITS && (2 << bits) <= len) ++bits;  // about one or two keys a sub-range
+    }
+    const int nb = 1 << bits;
+    const int per = nb >= 2048 ? nb / 1024 : 2;  // counters a thread scans and sorts (even)
+    const int owners = nb / per;
+    const float scale = large ? 0.f : (float)nb / __ull2float_ru(kmax - kmin);
+    auto digit = [&](unsigned long long k) { return min(nb - 1, (int)(__ull2float_rz(k - kmin) * scale)); };
+    if (!large) {
+        // pass 2: counts per sub-range
+        for (int w = tid; w < nb / 2; w += 1024) wd[w] = 0u;
+        __syncthreads();
+        msd_for_keys<U>(src, len, [&](int, U v) {
+            const int d = digit((unsigned long long)to_key<U, XF>(v));
+            atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16));
+        });
+        __syncthreads();
+        // exclusive scan of the counters (each owner a run of `per`), their largest
+        unsigned int sum = 0, m = 0;
+        if (tid < owners)
+            for (int q = 0; q < per / 2; ++q) {
+                const unsigned int w = wd[tid * (per / 2) + q];
+                sum += (w & 0xffffu) + (w >> 16);
+                m = max(m, max(w & 0xffffu, w >> 16));
+            }
+        unsigned int x = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 31) warp_tot[warp] = (int)x;
+        if (lane == 0) atomicMax(reinterpret_cast<unsigned int*>(&red[2]), m);
+        __syncthreads();
+        unsigned int run = x - sum;
+        for (int w = 0; w < warp; ++w) run += (unsigned int)warp_tot[w];
+        if (tid < owners)
+            for (int q = 0; q < per / 2; ++q) {
+                const unsigned int w = wd[tid * (per / 2) + q];
+                const unsigned int s0 = run, s1 = run + (w & 0xffffu);
+                run = s1 + (w >> 16);
+                wd[tid * (per / 2) + q] = s0 | (s1 << 16);  // starts, which become cursors
+            }
+        __syncthreads();
+        large = reinterpret_cast<unsigned int*>(&red[2])[0] > (unsigned int)MSD_SUB_MAX;
+        __syncthreads();
+        if (tid == 0) red[2] = 0ull;
+    }
+    if (large) {
+        seg_large_sort<U, XF>(src, dst, scratch, len, sk, l_cnt, warp_tot, &red[3], l_hist, l_run, l_run + 256,
+                              l_run + 512);
+        __syncthreads();
+        return;
+    }
+    // pass 3: place keys by sub-range; each counter ends at its sub-range's end
+    msd_for_keys<U>(src, len, [&](int, U v) {
+        const U k = to_key<U, XF>(v);
+        const int d = digit((unsigned long long)k);
+        sk[half(atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16)), d)] = k;
+    });
+    __syncthreads();
+    // pass 4: every owner insertion-sorts its run of sub-ranges
+    if (tid < owners) {
+        const int d0 = tid * per;
+        const int r0 = d0 == 0 ? 0 : (int)half(wd[(d0 - 1) >> 1], d0 - 1);
+        const int r1 = (int)half(wd[(d0 + per - 1) >> 1], d0 + per - 1);
+        for (int i = r0 + 1; i < r1; ++i) {
+            const U v = sk[i];
+            int j = i - 1;
+            while (j >= r0 && sk[j] > v) {
+                sk[j + 1] = sk[j];
+                --j;
+            }
+            sk[j + 1] = v;
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < len; i += 1024) dst[i] = from_key<U, XF>(sk[i]);
+    __syncthreads();
+}
+
 // ---- the persistent launch ---------------------------------------------------
 struct SegMethods {
     int m[SEG_BLOCK_BINS];
@@ -355,13 +533,10 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
     k_seg_sort(const U* data_in, U* data, U* __restrict__ alt, const unsigned long long* __restrict__ offsets,
                const unsigned int* __restrict__ lists, size_t n_seg, const SegPlan* __restrict__ plan,
                unsigned int* __restrict__ counter, SegMethods methods) {
+    static_assert(SegSmem::bytes<U>() <= (size_t)MSD_SMEM, "the on-chip sorts' areas fit the launch's shared memory");
     extern __shared__ __align__(128) unsigned char smem[];
     U* sm = reinterpret_cast<U*>(smem);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(smem + SegSmem::cnt_off<U>());
-    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + SegSmem::hist_off<U>());
-    uint32_t* run = reinterpret_cast<uint32_t*>(smem + SegSmem::run_off<U>());
-    uint32_t* lst = run + 256;
-    uint32_t* tcnt = run + 512;
     int* misc = reinterpret_cast<int*>(smem + SegSmem::misc_off<U>());
     int* warp_tot = misc;                                            // [32]
     unsigned long long* red = reinterpret_cast<unsigned long long*>(misc + 32);
@@ -389,8 +564,14 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
             const unsigned long long b = offsets[s];
             const int len = (int)(offsets[s + 1] - b);
             if (bin == SEG_BIN_LARGE) {
-                seg_large_sort<U, XF>(data_in + b, data + b, alt + b, len, sm, cnt, warp_tot, red, hist, run, lst,
-                                      tcnt);
+                if constexpr (sizeof(U) >= 4) {
+                    msd_sort<U, XF>(data_in + b, data + b, alt + b, len, smem);
+                } else {  // 8- and 16-bit keys crowd the sub-ranges: straight to the CTA-level LSD
+                    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + SegSmem::hist_off<U>());
+                    uint32_t* run = reinterpret_cast<uint32_t*>(smem + SegSmem::run_off<U>());
+                    seg_large_sort<U, XF>(data_in + b, data + b, alt + b, len, sm, cnt, warp_tot, red, hist, run,
+                                          run + 256, run + 512);
+                }
             } else {
                 const int m = methods.m[bin];
                 if (m == SEG_BITONIC) seg_block_bitonic<U, XF>(data_in + b, data + b, len, sm);

@@ -53,7 +53,7 @@ ts_status seg_prepare(ts_ctx* c, size_t n, size_t n_seg) {
     ts_status s;
     if ((s = grow(c, c->alt, n * sizeof(U) + 16, "segment scratch")) != TS_OK) return s;
     if ((s = grow(c, c->seg, SegLayout::make(n_seg).bytes, "segment lists")) != TS_OK) return s;
-    occupancy_of((const void*)k_seg_sort<U, XF>, SEG_THREADS, SegSmem::bytes<U>());
+    occupancy_of((const void*)k_seg_sort<U, XF>, SEG_THREADS, MSD_SMEM);
     return TS_OK;
 }
 
@@ -70,7 +70,7 @@ ts_status seg_enqueue(ts_ctx* c, U* d, size_t n, const unsigned long long* d_off
     const int grid = (int)std::min<size_t>((n_seg + 255) / 256, (size_t)c->sm_count * 8);
     k_seg_bin_max<U, XF><<<std::max(grid, 1), 256, 0, c->stream>>>(d_off, n_seg, n, max_len, plan, lists, c->d_error);
     k_seg_items<<<1, 32, 0, c->stream>>>(plan);
-    k_seg_sort<U, XF><<<c->sm_count, SEG_THREADS, SegSmem::bytes<U>(), c->stream>>>(d, d, (U*)c->alt.p, d_off,
+    k_seg_sort<U, XF><<<c->sm_count, SEG_THREADS, MSD_SMEM, c->stream>>>(d, d, (U*)c->alt.p, d_off,
                                                                                      lists, n_seg, plan, counter, m);
     c->launches += 3;
     TS_CUDA(c, cudaGetLastError());
