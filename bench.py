@@ -9,7 +9,9 @@ pass, finishing kernels) of 2^28 keys already resident in HBM (1 GiB, far
 above the 126 MB L2); each step sorts its own unsorted copy. `value` is keys
 sorted per second over the K timed steps (CUDA events on the sort's stream,
 max over ranks). `e2e` times the host-slice C ABI call ts_sort_u32 on pinned
-host memory: the copy in, the sort and the copy out. `roofline` is the
+host memory: the copy in, the sort and the copy out, which the library
+overlaps (chunked copies in, chunk sorts and device merges, sliced copies
+out); the same call with the copies serialised is reported beside it. `roofline` is the
 onesweep pass kernel: algorithmic bytes of one pass (read + write of every
 key) over its CUDA-event duration, against the measured HBM copy bandwidth.
 Under torchrun each rank sorts its own array (replicas: the crate's sort has
@@ -235,6 +237,10 @@ def workload_config(name: str, lg: int | None = None) -> dict:
             "name": name, "n": 1 << lg, "key_type": kind,
             "l2": "inputs larger than L2 (1 GiB vs 126 MB); each step sorts its own unsorted copy",
             "parallelism": "replicas"}
+
+
+PIPE_CHUNKS = 8            # the library's default transfer pipeline
+PIPE_MIN_BYTES = 64 << 20
 
 
 def reduce_over_ranks(torch, dist_mod, ms: float, ok: bool, device: str) -> tuple[float, bool]:
@@ -627,33 +633,48 @@ def main() -> None:
         "clocks": clk,
     }
 
-    # end to end through the host-slice C ABI call, pinned host memory
+    # end to end through the host-slice C ABI call, pinned host memory: the
+    # library's default (copies overlapped with chunk sorts and merges), then
+    # the same call with the copies serialised, for comparison
     if not args.no_e2e:
         host = gen(kind, dist, n, 0x9E3779B97F4A7C15 + rank)
         pinned = torch.empty(n * w, dtype=torch.uint8, pin_memory=True).numpy().view(NP[kind])
-        e_ms = []
-        for i in range(args.warmup + args.steps):
-            np.copyto(pinned, host)
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            ts.sort(pinned, ctx)
-            e1.record()
-            torch.cuda.synchronize()
-            if i >= args.warmup:
-                e_ms.append(e0.elapsed_time(e1))
-        emax = sum(e_ms)
-        if dist_mod is not None:
-            t = torch.tensor([emax], dtype=torch.float64, device=f"cuda:{local}")
-            dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
-            emax = float(t.item())
         s_ref, x_ref = checksums(host)
+
+        def host_calls(steps):
+            e_ms, ok = [], True
+            for i in range(args.warmup + steps):
+                np.copyto(pinned, host)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                ts.sort(pinned, ctx)
+                e1.record()
+                torch.cuda.synchronize()
+                if i >= args.warmup:
+                    e_ms.append(e0.elapsed_time(e1))
+            ok = check_sorted(pinned, s_ref, x_ref)
+            total = sum(e_ms)
+            if dist_mod is not None:
+                t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
+                dist_mod.all_reduce(t, op=dist_mod.ReduceOp.MAX)
+                total = float(t.item())
+            return total, ok
+
+        ctx.transfer_pipeline(PIPE_CHUNKS, PIPE_MIN_BYTES)
+        emax, ok = host_calls(args.steps)
+        serial_steps = max(1, min(args.steps, 5))
+        ctx.transfer_pipeline(1, PIPE_MIN_BYTES)
+        smax, sok = host_calls(serial_steps)
+        ctx.transfer_pipeline(PIPE_CHUNKS, PIPE_MIN_BYTES)
         line["e2e"] = {"value": round(world * n * args.steps / (emax / 1e3) / 1e9, 3), "unit": "GKeys/s",
                        "h2d_bytes_per_step": n * w, "d2h_bytes_per_step": n * w,
                        "ms_per_step": round(emax / args.steps, 3),
                        "call": f"ts_sort_{kind} on pinned host memory",
-                       "bit_exact_checks": "sorted + sum/xor" if check_sorted(pinned, s_ref, x_ref) else "FAILED"}
+                       "pipeline": {"chunks": PIPE_CHUNKS, "min_bytes": PIPE_MIN_BYTES,
+                                    "serial_ms_per_step": round(smax / serial_steps, 3)},
+                       "bit_exact_checks": "sorted + sum/xor" if ok and sok else "FAILED"}
         del pinned
 
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -60,6 +60,14 @@ ts_status ts_ctx_reserve(ts_ctx *ctx, size_t n, size_t key_bytes, int with_order
 /* Elements of `key_bytes` the context can sort without growing
  * (SortByKeyBuffer::capacity, src/by_key.rs:84-90). */
 size_t ts_ctx_capacity(const ts_ctx *ctx, size_t key_bytes, int with_order);
+/* Host-slice sorts (ts_sort_<T>, ts_sort_with_buffer_<T>, ts_sort_parallel_<T>;
+ * keys of 2 bytes or more) of at least `min_bytes` cross PCIe as `chunks`
+ * pieces (a power of two, 1 to 64) on a second stream: each piece is sorted
+ * while the next one is in flight, the sorted pieces are merged pairwise on
+ * the device, and the last merge's output is copied back slice by slice
+ * while the rest is merged. chunks = 1 copies in, sorts and copies out. The
+ * output is the same either way. Default: 8 chunks from 64 MiB. */
+ts_status ts_ctx_transfer_pipeline(ts_ctx *ctx, int chunks, size_t min_bytes);
 const char *ts_ctx_last_error(const ts_ctx *ctx);
 const char *ts_status_str(ts_status s);
 
@@ -113,8 +121,10 @@ ts_status ts_apply_order_dev(ts_ctx *ctx, void *d_data, size_t n, size_t elem_si
  * data[offsets[i] .. offsets[i+1]) in place, independently, for i < n_seg;
  * offsets holds n_seg + 1 non-decreasing entries ending within n. One device
  * launch sorts the whole batch: segments are binned by length (32 keys and
- * fewer: a warp each; up to 16384 (8192 for 8-byte keys): on chip; longer: a CTA each through L2;
- * host calls send segments above 2^22 keys to the device-wide sort). The _dev
+ * fewer: a warp each; up to 16384 (8192 for 8-byte keys): on chip; longer: a
+ * CTA each, by one MSD pass in shared memory up to 49.6K 4-byte or 24.8K
+ * 8-byte keys, else by an LSD through L2; host calls send segments above 2^22
+ * keys to the device-wide sort). The _dev
  * form replays a captured CUDA graph when called again with the same
  * pointers and sizes. Segments must hold fewer than 2^31 keys. */
 #define TS_DECLARE_SEGMENTS(SUF, T)                                                                       \

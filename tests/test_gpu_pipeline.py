@@ -1,0 +1,114 @@
+"""Parity of the host-slice sort with its copies overlapped (chunked copies
+in, chunk sorts, pairwise device merges, sliced copies out) with the oracle,
+through the C ABI. Every comparison is bit-exact; the pipeline is forced on
+at small sizes by setting its size threshold to zero.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+PIPE_TYPES = [t for t in O.TYPES if t not in ("u8", "i8")]
+
+
+@pytest.fixture(scope="module")
+def ts():
+    import turbosort_b200 as ts
+
+    return ts
+
+
+def gen(t, n, shape, rng):
+    kd = O.KEY_DTYPE[t]
+    b = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+    if shape == "few":
+        b %= np.uint64(7)
+    elif shape == "const":
+        b[:] = b[0]
+    a = b.astype(kd).view(O.NP_DTYPE[t])
+    if shape == "asc":
+        a = O.sort(a)
+    elif shape == "desc":
+        a = O.sort(a)[::-1].copy()
+    if t in ("f32", "f64") and shape == "random":
+        ft = np.float32 if t == "f32" else np.float64
+        sp = np.array([np.nan, -np.nan, np.inf, -np.inf, 0.0, -0.0], dtype=ft)
+        idx = rng.integers(0, n, size=max(1, n // 50))
+        a[idx] = sp[rng.integers(0, sp.size, size=idx.size)]
+    return a
+
+
+def run(ts, ctx, a):
+    got = a.copy()
+    ts.sort(got, ctx)
+    return got
+
+
+@pytest.mark.parametrize("t", PIPE_TYPES)
+def test_pipeline_matches_oracle(ts, t):
+    ctx = ts.Context(0)
+    rng = np.random.default_rng(abs(hash(("pipe", t))) % 2**32)
+    for chunks in (2, 8, 64):
+        ctx.transfer_pipeline(chunks, 0)
+        for n in (chunks * 256, chunks * 256 + 1, 100_003, (1 << 20) + 17):
+            for shape in ("random", "few", "asc", "desc", "const"):
+                a = gen(t, n, shape, rng)
+                got = run(ts, ctx, a)
+                assert got.tobytes() == O.sort(a).tobytes(), (t, chunks, n, shape)
+    ctx.close()
+
+
+def test_pipeline_runs_merges_and_agrees_with_serial(ts):
+    ctx = ts.Context(0)
+    rng = np.random.default_rng(3)
+    a = gen("u32", 3_000_001, "random", rng)
+    ctx.transfer_pipeline(1, 0)
+    serial = run(ts, ctx, a)
+    ctx.transfer_pipeline(8, 0)
+    ctx.reset_timings()
+    ctx.enable_timing(True)
+    before = ts.lib().ts_ctx_launches(ctx.handle)
+    piped = run(ts, ctx, a)
+    ctx.enable_timing(False)
+    assert "merge" in ctx.timings()
+    # 8 chunk sorts, 7 merges: each merge is a split launch plus tile launches
+    assert ts.lib().ts_ctx_launches(ctx.handle) - before >= 8 + 14
+    assert piped.tobytes() == serial.tobytes() == O.sort(a).tobytes()
+    ctx.close()
+
+
+def test_default_threshold_and_repeated_calls(ts):
+    """2^24 u32 keys (64 MiB) reach the default threshold; repeated and
+    differently sized calls on one context reuse and grow its buffers."""
+    ctx = ts.Context(0)
+    rng = np.random.default_rng(5)
+    for n in (1 << 24, 1 << 24, (1 << 22) + 3, (1 << 24) + 4097):
+        a = gen("u32", n, "random", rng)
+        ctx.transfer_pipeline(8, 0 if n < (1 << 24) else 64 << 20)
+        assert run(ts, ctx, a).tobytes() == O.sort(a).tobytes(), n
+    ctx.close()
+
+
+def test_pinned_host_slice(ts):
+    import torch
+
+    ctx = ts.Context(0)
+    ctx.transfer_pipeline(16, 0)
+    rng = np.random.default_rng(9)
+    for t, n in (("f32", 2_000_003), ("i64", 1_000_033)):
+        a = gen(t, n, "random", rng)
+        pinned = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(a.dtype)
+        np.copyto(pinned, a)
+        ts.sort(pinned, ctx)
+        assert pinned.tobytes() == O.sort(a).tobytes(), t
+    ctx.close()
+
+
+def test_rejects_bad_chunk_counts(ts):
+    ctx = ts.Context(0)
+    for bad in (0, 3, 12, 128):
+        with pytest.raises(ts.TurbosortError):
+            ctx.transfer_pipeline(bad, 0)
+    ctx.close()

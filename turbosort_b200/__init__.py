@@ -142,6 +142,8 @@ def lib() -> ctypes.CDLL:
             L.ts_segments_autotune.restype = st
             L.ts_segments_methods.argtypes = [vp, sz, vp, i]
             L.ts_segments_methods.restype = st
+            L.ts_ctx_transfer_pipeline.argtypes = [vp, i, sz]
+            L.ts_ctx_transfer_pipeline.restype = st
             L.ts_ctx_use_graphs.argtypes = [vp, i]
             L.ts_ctx_use_graphs.restype = st
             L.ts_ctx_launches.argtypes = [vp]
@@ -207,6 +209,11 @@ class Context:
 
     def capacity(self, key_bytes: int, with_order: bool = False) -> int:
         return int(lib().ts_ctx_capacity(self._h, key_bytes, int(with_order)))
+
+    def transfer_pipeline(self, chunks: int = 8, min_bytes: int = 64 << 20) -> None:
+        """Host-slice sorts of at least min_bytes cross PCIe as `chunks` pieces,
+        sorted and merged on the device while the copies run (1 turns it off)."""
+        self._check(lib().ts_ctx_transfer_pipeline(self._h, chunks, min_bytes))
 
     def enable_timing(self, on: bool = True) -> None:
         self._check(lib().ts_ctx_enable_timing(self._h, int(on)))

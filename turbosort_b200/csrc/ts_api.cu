@@ -112,6 +112,10 @@ static ts_status host_sort(ts_ctx* c, T* data, size_t n) {
     if (!c) return TS_ERR_INVALID;
     if (n <= 1) return TS_OK;
     if (!data) return fail(c, TS_ERR_INVALID, "null data");
+    if constexpr (sizeof(U) > 1) {
+        if (c->transfer_chunks > 1 && n * sizeof(U) >= c->transfer_min_bytes && n >= (size_t)c->transfer_chunks * 256)
+            return pipeline_sort<U, XF>(c, (U*)data, n);
+    }
     ts_status s;
     if ((s = grow(c, c->keys, n * sizeof(U), "keys")) != TS_OK) return s;
     U* d = (U*)c->keys.p;
@@ -230,8 +234,12 @@ void ts_ctx_destroy(ts_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg, &c->learn})
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg,
+                      &c->learn, &c->pipe})
         if (b->p) cudaFree(b->p);
+    for (auto ev : c->pipe_events) cudaEventDestroy(ev);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->seg_graph) cudaGraphExecDestroy(c->seg_graph);
     if (c->sort_graph) cudaGraphExecDestroy(c->sort_graph);
     if (c->d_error) cudaFree(c->d_error);
@@ -251,6 +259,15 @@ ts_status ts_ctx_set_stream(ts_ctx* c, void* stream) {
 }
 
 void* ts_ctx_stream(ts_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+ts_status ts_ctx_transfer_pipeline(ts_ctx* c, int chunks, size_t min_bytes) {
+    if (!c) return TS_ERR_INVALID;
+    if (chunks < 1 || chunks > 64 || (chunks & (chunks - 1)) != 0)
+        return fail(c, TS_ERR_INVALID, "transfer chunks must be a power of two from 1 to 64");
+    c->transfer_chunks = chunks;
+    c->transfer_min_bytes = min_bytes;
+    return TS_OK;
+}
 
 ts_status ts_ctx_synchronize(ts_ctx* c) {
     if (!c) return TS_ERR_INVALID;

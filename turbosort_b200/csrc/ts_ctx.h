@@ -37,6 +37,7 @@ struct ts_ctx {
     ts::DevBuf gather;             // apply_order staging
     ts::DevBuf seg;                // segmented sort: plan, work counter, bin lists, offsets
     ts::DevBuf learn;              // learned partition: sample, model, training state, bucket counts
+    ts::DevBuf pipe;               // host-slice pipeline: merge split points
     uint32_t* d_error = nullptr;   // kernel-reported errors, read and cleared by the host
 
     // segmented sort: the method of each on-chip length bin per key width
@@ -52,6 +53,13 @@ struct ts_ctx {
     size_t sort_graph_key[8] = {};
     size_t sort_last_key[8] = {};
     unsigned long long sort_graph_launches = 0;
+
+    // host-slice sorts of at least transfer_min_bytes cross as transfer_chunks
+    // pieces on copy_stream, sorted and merged while the copies run
+    int transfer_chunks = 8;
+    size_t transfer_min_bytes = (size_t)64 << 20;
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t> pipe_events;
 
     std::string last_error;
     unsigned long long launches = 0;   // kernels this context has launched
@@ -81,6 +89,9 @@ template <typename U, int XF>
 ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt);
 template <typename U, int XF>
 ts_status order_device(ts_ctx* c, const U* d_keys, size_t n, uint32_t* d_order);
+// The host slice h[0, n) sorted with its copies overlapped; returns when done.
+template <typename U, int XF>
+ts_status pipeline_sort(ts_ctx* c, U* h, size_t n);
 
 }  // namespace ts
 

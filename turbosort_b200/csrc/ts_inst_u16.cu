@@ -1,10 +1,13 @@
 // Instantiates the device sorts for 16-bit keys: unsigned, signed and (for
 // 32/64 bits) IEEE float transforms.
 #include "ts_engine.cuh"
+#include "ts_pipeline.cuh"
 
 namespace ts {
 template ts_status sort_keys_device<uint16_t, 0>(ts_ctx*, uint16_t*, size_t, uint16_t*);
 template ts_status sort_keys_device<uint16_t, 1>(ts_ctx*, uint16_t*, size_t, uint16_t*);
 template ts_status order_device<uint16_t, 0>(ts_ctx*, const uint16_t*, size_t, uint32_t*);
 template ts_status order_device<uint16_t, 1>(ts_ctx*, const uint16_t*, size_t, uint32_t*);
+template ts_status pipeline_sort<uint16_t, 0>(ts_ctx*, uint16_t*, size_t);
+template ts_status pipeline_sort<uint16_t, 1>(ts_ctx*, uint16_t*, size_t);
 }  // namespace ts

@@ -1,6 +1,7 @@
 // Instantiates the device sorts for 32-bit keys: unsigned, signed and (for
 // 32/64 bits) IEEE float transforms.
 #include "ts_engine.cuh"
+#include "ts_pipeline.cuh"
 
 namespace ts {
 template ts_status sort_keys_device<uint32_t, 0>(ts_ctx*, uint32_t*, size_t, uint32_t*);
@@ -9,4 +10,7 @@ template ts_status order_device<uint32_t, 0>(ts_ctx*, const uint32_t*, size_t, u
 template ts_status order_device<uint32_t, 1>(ts_ctx*, const uint32_t*, size_t, uint32_t*);
 template ts_status sort_keys_device<uint32_t, 2>(ts_ctx*, uint32_t*, size_t, uint32_t*);
 template ts_status order_device<uint32_t, 2>(ts_ctx*, const uint32_t*, size_t, uint32_t*);
+template ts_status pipeline_sort<uint32_t, 0>(ts_ctx*, uint32_t*, size_t);
+template ts_status pipeline_sort<uint32_t, 1>(ts_ctx*, uint32_t*, size_t);
+template ts_status pipeline_sort<uint32_t, 2>(ts_ctx*, uint32_t*, size_t);
 }  // namespace ts
