@@ -106,6 +106,18 @@ def test_pinned_host_slice(ts):
     ctx.close()
 
 
+def test_pageable_slice_larger_than_the_staging_ring(ts):
+    """A pageable slice goes through four pinned 32 MiB slots; 512 MiB of u64
+    keys in two chunks wraps the ring several times each way."""
+    ctx = ts.Context(0)
+    ctx.transfer_pipeline(2, 0)
+    rng = np.random.default_rng(11)
+    a = gen("u64", (1 << 26) + 12345, "random", rng)
+    got = run(ts, ctx, a)
+    assert got.tobytes() == O.sort(a).tobytes()
+    ctx.close()
+
+
 def test_rejects_bad_chunk_counts(ts):
     ctx = ts.Context(0)
     for bad in (0, 3, 12, 128):

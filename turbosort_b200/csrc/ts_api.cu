@@ -10,6 +10,7 @@
 
 #include "ts_ctx.h"
 #include "ts_gather.cuh"
+#include "ts_staging.h"
 
 namespace ts {
 
@@ -239,7 +240,10 @@ void ts_ctx_destroy(ts_ctx* c) {
                       &c->learn, &c->pipe})
         if (b->p) cudaFree(b->p);
     for (auto ev : c->pipe_events) cudaEventDestroy(ev);
+    for (auto ev : c->stage_events) cudaEventDestroy(ev);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->stage) cudaFreeHost(c->stage);
+    delete c->copy_pool;
     if (c->seg_graph) cudaGraphExecDestroy(c->seg_graph);
     if (c->sort_graph) cudaGraphExecDestroy(c->sort_graph);
     if (c->d_error) cudaFree(c->d_error);

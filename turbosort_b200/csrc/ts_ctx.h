@@ -19,6 +19,7 @@ struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
 };
+class CopyPool;
 
 }  // namespace ts
 
@@ -60,6 +61,11 @@ struct ts_ctx {
     size_t transfer_min_bytes = (size_t)64 << 20;
     cudaStream_t copy_stream = nullptr;
     std::vector<cudaEvent_t> pipe_events;
+    // pageable host slices go through pinned staging slots, filled and
+    // emptied by the copy pool's threads
+    void* stage = nullptr;                 // pinned host memory: STAGE_SLOTS slots
+    std::vector<cudaEvent_t> stage_events; // the last DMA of each slot
+    ts::CopyPool* copy_pool = nullptr;
 
     std::string last_error;
     unsigned long long launches = 0;   // kernels this context has launched

@@ -17,8 +17,14 @@
 // scratch a chunk sort takes (Y over the chunk's range) and the target of
 // every merge never overlap a live run. Host calls are ordered so that the
 // copy of chunk i + 2 is issued after the sort of chunk i and every copy out
-// after the last merge: a pageable host slice, whose copies hold the host
-// thread, still overlaps the GPU work already queued.
+// after the last merge.
+//
+// A pageable host slice cannot be a DMA source or target; the driver would
+// copy it through its own pinned buffer on this thread at about a quarter of
+// the PCIe rate. Such a slice goes through the context's pinned staging
+// slots instead: the copy pool's threads fill a slot while the DMA of the
+// previous one runs, and on the way back empty a slot while the next one's
+// DMA runs.
 #pragma once
 
 #include <algorithm>
@@ -26,10 +32,35 @@
 
 #include "ts_engine.cuh"
 #include "ts_merge.cuh"
+#include "ts_staging.h"
 
 namespace ts {
 
-constexpr int PIPE_SLICES = 8;  // output slices of the last merge
+constexpr int PIPE_SLICES = 8;                     // output slices of the last merge
+constexpr int STAGE_SLOTS = 4;                     // pinned staging slots for pageable slices
+constexpr size_t STAGE_SLOT_BYTES = (size_t)32 << 20;
+
+// the pinned slots, their events and the copy threads; false if pinned
+// memory cannot be had (the slice then takes the driver's own staging)
+inline bool stage_resources(ts_ctx* c) {
+    if (!c->stage) {
+        if (cudaHostAlloc(&c->stage, STAGE_SLOTS * STAGE_SLOT_BYTES, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            c->stage = nullptr;
+            return false;
+        }
+    }
+    while (c->stage_events.size() < (size_t)STAGE_SLOTS) {
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        c->stage_events.push_back(ev);
+    }
+    if (!c->copy_pool) c->copy_pool = new CopyPool(copy_pool_workers());
+    return true;
+}
 
 // the copy stream and the events a pipelined call uses, made once per context
 inline ts_status pipe_resources(ts_ctx* c, size_t events) {
@@ -80,6 +111,27 @@ ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
     if ((s = grow(c, c->pipe, ((n + MERGE_TILE - 1) / MERGE_TILE + 1) * sizeof(size_t), "merge splits")) != TS_OK)
         return s;
     if ((s = pipe_resources(c, (size_t)C + PIPE_SLICES + 2)) != TS_OK) return s;
+    cudaPointerAttributes pa{};
+    bool pageable = cudaPointerGetAttributes(&pa, h) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered;
+    cudaGetLastError();
+    if (pageable && !stage_resources(c)) pageable = false;
+    char* stage = (char*)c->stage;
+    int slot = 0;
+    // staged copy in of h[b, e): each slot waits for its previous DMA, is
+    // filled by the copy threads, then goes to the device
+    auto staged_in = [&](U* dst, const U* src, size_t count) -> ts_status {
+        const size_t per = STAGE_SLOT_BYTES / sizeof(U);
+        for (size_t q = 0; q < count; q += per) {
+            const size_t m = std::min(per, count - q);
+            TS_CUDA(c, cudaEventSynchronize(c->stage_events[slot]));
+            char* buf = stage + (size_t)slot * STAGE_SLOT_BYTES;
+            c->copy_pool->copy(buf, src + q, m * sizeof(U));
+            TS_CUDA(c, cudaMemcpyAsync(dst + q, buf, m * sizeof(U), cudaMemcpyHostToDevice, c->copy_stream));
+            TS_CUDA(c, cudaEventRecord(c->stage_events[slot], c->copy_stream));
+            slot = (slot + 1) % STAGE_SLOTS;
+        }
+        return TS_OK;
+    };
     U* X = (U*)c->keys.p;
     U* Y = (U*)c->alt.p;
     const size_t chunk = ((n + C - 1) / C + 255) / 256 * 256;  // chunk starts 256 keys apart: 16-byte aligned
@@ -95,8 +147,14 @@ ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
     auto copy_in = [&](int i) -> ts_status {
         if (i >= C) return TS_OK;
         const size_t b = lo(i), e = lo(i + 1);
-        if (e > b)
-            TS_CUDA(c, cudaMemcpyAsync(X + b, h + b, (e - b) * sizeof(U), cudaMemcpyHostToDevice, c->copy_stream));
+        if (e > b) {
+            if (pageable) {
+                ts_status st = staged_in(X + b, h + b, e - b);
+                if (st != TS_OK) return st;
+            } else {
+                TS_CUDA(c, cudaMemcpyAsync(X + b, h + b, (e - b) * sizeof(U), cudaMemcpyHostToDevice, c->copy_stream));
+            }
+        }
         TS_CUDA(c, cudaEventRecord(in_ev[i], c->copy_stream));
         return TS_OK;
     };
@@ -136,13 +194,49 @@ ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
     }
     mark(c, "end");
     // the sorted slice goes back one merged output slice at a time
-    size_t from = 0;
-    for (int p = 0; p < PIPE_SLICES; ++p) {
-        TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, out_ev[p], 0));
-        if (slice_end[p] > from)
-            TS_CUDA(c, cudaMemcpyAsync(h + from, final_buf + from, (slice_end[p] - from) * sizeof(U),
+    if (!pageable) {
+        size_t from = 0;
+        for (int p = 0; p < PIPE_SLICES; ++p) {
+            TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, out_ev[p], 0));
+            if (slice_end[p] > from)
+                TS_CUDA(c, cudaMemcpyAsync(h + from, final_buf + from, (slice_end[p] - from) * sizeof(U),
+                                           cudaMemcpyDeviceToHost, c->copy_stream));
+            from = std::max(from, slice_end[p]);
+        }
+    } else {
+        // pieces of at most one slot, none across a slice end; the DMA of
+        // piece k + STAGE_SLOTS - 1 is queued before the threads empty piece k
+        struct Piece {
+            size_t b, e;
+            int slice;
+        };
+        std::vector<Piece> pieces;
+        const size_t per = STAGE_SLOT_BYTES / sizeof(U);
+        size_t from = 0;
+        for (int p = 0; p < PIPE_SLICES; ++p) {
+            for (size_t q = from; q < slice_end[p]; q += per) pieces.push_back({q, std::min(slice_end[p], q + per), p});
+            from = std::max(from, slice_end[p]);
+        }
+        int waited = -1;  // the last slice the copy stream waits for
+        auto issue = [&](size_t k) -> ts_status {
+            const Piece& pc = pieces[k];
+            for (; waited < pc.slice; ++waited) TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, out_ev[waited + 1], 0));
+            const int sl = (int)(k % STAGE_SLOTS);
+            TS_CUDA(c, cudaMemcpyAsync(stage + (size_t)sl * STAGE_SLOT_BYTES, final_buf + pc.b, (pc.e - pc.b) * sizeof(U),
                                        cudaMemcpyDeviceToHost, c->copy_stream));
-        from = std::max(from, slice_end[p]);
+            TS_CUDA(c, cudaEventRecord(c->stage_events[sl], c->copy_stream));
+            return TS_OK;
+        };
+        for (size_t k = 0; k + 1 < (size_t)STAGE_SLOTS && k < pieces.size(); ++k)
+            if ((s = issue(k)) != TS_OK) return s;
+        for (size_t k = 0; k < pieces.size(); ++k) {
+            if (k + STAGE_SLOTS - 1 < pieces.size())
+                if ((s = issue(k + STAGE_SLOTS - 1)) != TS_OK) return s;
+            const int sl = (int)(k % STAGE_SLOTS);
+            TS_CUDA(c, cudaEventSynchronize(c->stage_events[sl]));
+            c->copy_pool->copy(h + pieces[k].b, stage + (size_t)sl * STAGE_SLOT_BYTES,
+                               (pieces[k].e - pieces[k].b) * sizeof(U));
+        }
     }
     TS_CUDA(c, cudaEventRecord(done_ev, c->copy_stream));
     TS_CUDA(c, cudaStreamWaitEvent(c->stream, done_ev, 0));
