@@ -34,3 +34,17 @@ def test_cpp_api_examples(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == "ok"
+
+
+def test_copy_pool_copies_every_byte(tmp_path):
+    """The transfer pipeline's host copy threads (ts_staging.h), on the CPU."""
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    exe = str(tmp_path / "copy_pool_test")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-pthread", "-I", os.path.join(ROOT, "turbosort_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cpp", "copy_pool_test.cpp"), "-o", exe],
+                   check=True, capture_output=True, text=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.strip() == "ok"
