@@ -187,10 +187,27 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
 
     uint32_t parity = 0;  // bit b: the phase buffer b's barrier completes next
 
+    // The first live pass transforms keys as it loads them (and makes the
+    // positions), the last undoes the transform as it writes. For float keys
+    // and for pairs that is a compile-time choice (TAGGED: the tile body is
+    // built for both); a signed key's transform is one XOR, done with a mask
+    // that is the sign bit only in the first or last pass.
+    constexpr bool TAGGED = XF == 2 || PAIRS;
+    constexpr U SIGN = (U)((U)1 << (8 * sizeof(U) - 1));
+    const U first_mask = (XF == 1 && first) ? SIGN : (U)0;
+    const U last_mask = (XF == 1 && last) ? SIGN : (U)0;
+
     // One tile. FULL (a compile-time tag) drops every per-key bounds test:
-    // only the last tile of a portion can be partial.
-    auto process = [&](int t, int b, auto full_tag) {
+    // only the last tile of a portion can be partial. FIRST is the
+    // compile-time first-pass tag (false unless TAGGED).
+    auto process = [&](int t, int b, auto full_tag, auto first_tag) {
         constexpr bool FULL = decltype(full_tag)::value;
+        constexpr bool FIRST = decltype(first_tag)::value;
+        auto load_key = [&](U k) -> U {
+            if constexpr (FIRST) return to_key<U, XF>(k);
+            else if constexpr (XF == 1 && !TAGGED) return (U)(k ^ first_mask);
+            else return k;
+        };
         const size_t tile_base = a.portion_begin + (size_t)t * TILE;
         const int tile_n = FULL ? TILE : (int)min((size_t)TILE, portion_end - tile_base);
         U* kb = kbuf + (size_t)b * TILE;
@@ -216,8 +233,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
 #pragma unroll
             for (int i = 0; i < IPT; ++i) {
                 if (FULL || wbase + i * 32 < tile_n) {
-                    U k = kb[wbase + i * 32];
-                    if (first) k = to_key<U, XF>(k);
+                    const U k = load_key(kb[wbase + i * 32]);
                     atomicAdd(&my_cnt[digit_of(k, shift, MASK)], 1u);
                 }
             }
@@ -272,8 +288,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
             for (int i = 0; i < IPT; ++i) {
                 const int idx = wbase + i * 32;
                 const bool valid = FULL || idx < tile_n;
-                U k = kb[FULL ? idx : min(idx, TILE - 1)];
-                if (first) k = to_key<U, XF>(k);
+                const U k = load_key(kb[FULL ? idx : min(idx, TILE - 1)]);
                 const uint32_t d = digit_of(k, shift, MASK);
                 uint32_t peers;
                 if ((i % MATCH_MOD) < MATCH_CNT) peers = __match_any_sync(0xffffffffu, d);
@@ -284,7 +299,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                     my_cnt[d] = c + __popc(peers);
                     const uint32_t pos = c + __popc(peers & lt);
                     sk[pos] = k;
-                    if constexpr (PAIRS) sv[pos] = first ? (uint32_t)(tile_base + idx) : vb[idx];
+                    if constexpr (PAIRS) sv[pos] = FIRST ? (uint32_t)(tile_base + idx) : vb[idx];
                 }
                 __syncwarp();
             }
@@ -345,23 +360,46 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
         }
         __syncthreads();
 
-        // ---- 5. runs per digit to global memory
+        // ---- 5. runs per digit to global memory (the last live pass undoes
+        // the key transform as it writes)
+        auto scatter = [&](auto last_tag) {
+            constexpr bool LAST = decltype(last_tag)::value;
 #pragma unroll
-        for (int i = 0; i < SCATTER_IT; ++i) {
-            const int s = i * THREADS + tid;
-            if ((TILE % THREADS == 0 || i < SCATTER_IT - 1 || s < TILE) && (FULL || s < tile_n)) {
-                const U k = sk[s];
-                const OFF p = gbase[digit_of(k, shift, MASK)] + (OFF)s;
-                if (write_keys) dst[p] = last ? from_key<U, XF>(k) : k;
-                if constexpr (PAIRS) vdst[p] = sv[s];
+            for (int i = 0; i < SCATTER_IT; ++i) {
+                const int s = i * THREADS + tid;
+                if ((TILE % THREADS == 0 || i < SCATTER_IT - 1 || s < TILE) && (FULL || s < tile_n)) {
+                    const U k = sk[s];
+                    const OFF p = gbase[digit_of(k, shift, MASK)] + (OFF)s;
+                    if (write_keys) {
+                        if constexpr (LAST) dst[p] = from_key<U, XF>(k);
+                        else if constexpr (XF == 1) dst[p] = (U)(k ^ last_mask);
+                        else dst[p] = k;
+                    }
+                    if constexpr (PAIRS) vdst[p] = sv[s];
+                }
             }
+        };
+        if constexpr (XF == 2) {
+            if (last) scatter(std::true_type{});
+            else scatter(std::false_type{});
+        } else {
+            scatter(std::false_type{});
         }
         // clear the counters for the next tile (no one reads them past step 3)
         for (int i = tid; i < RANK_WARPS * RADIX; i += THREADS) cnt[i] = 0;
     };
     auto run_tile = [&](int t, int b) {
-        if (a.portion_begin + (size_t)(t + 1) * TILE <= portion_end) process(t, b, std::true_type{});
-        else process(t, b, std::false_type{});
+        const bool full = a.portion_begin + (size_t)(t + 1) * TILE <= portion_end;
+        auto go = [&](auto first_tag) {
+            if (full) process(t, b, std::true_type{}, first_tag);
+            else process(t, b, std::false_type{}, first_tag);
+        };
+        if constexpr (TAGGED) {
+            if (first) go(std::true_type{});
+            else go(std::false_type{});
+        } else {
+            go(std::false_type{});
+        }
     };
 
     if constexpr (NBUF == 2) {
