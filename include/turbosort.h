@@ -60,13 +60,16 @@ ts_status ts_ctx_reserve(ts_ctx *ctx, size_t n, size_t key_bytes, int with_order
 /* Elements of `key_bytes` the context can sort without growing
  * (SortByKeyBuffer::capacity, src/by_key.rs:84-90). */
 size_t ts_ctx_capacity(const ts_ctx *ctx, size_t key_bytes, int with_order);
-/* Host-slice sorts (ts_sort_<T>, ts_sort_with_buffer_<T>, ts_sort_parallel_<T>;
- * keys of 2 bytes or more) of at least `min_bytes` cross PCIe as `chunks`
- * pieces (a power of two, 1 to 64) on a second stream: each piece is sorted
- * while the next one is in flight, the sorted pieces are merged pairwise on
- * the device, and the last merge's output is copied back slice by slice
- * while the rest is merged. chunks = 1 copies in, sorts and copies out. The
- * output is the same either way. Default: 8 chunks from 64 MiB. */
+/* Host-slice sorts (ts_sort_<T>, ts_sort_with_buffer_<T>, ts_sort_parallel_<T>,
+ * and ts_sort_keys_order_<T> counting keys plus order; keys of 2 bytes or
+ * more) of at least `min_bytes` cross PCIe as `chunks` pieces (a power of
+ * two, 1 to 64) on a second stream: each piece is sorted (or ordered) while
+ * the next one is in flight, the pieces' results are merged pairwise on the
+ * device, and the last merge's output is copied back slice by slice while
+ * the rest is merged. A pageable host slice goes through pinned staging
+ * slots of the context, filled and emptied by host threads. chunks = 1
+ * copies in, sorts and copies out. The output is the same either way.
+ * Default: 8 chunks from 64 MiB. */
 ts_status ts_ctx_transfer_pipeline(ts_ctx *ctx, int chunks, size_t min_bytes);
 const char *ts_ctx_last_error(const ts_ctx *ctx);
 const char *ts_status_str(ts_status s);

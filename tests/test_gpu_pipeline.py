@@ -118,6 +118,43 @@ def test_pageable_slice_larger_than_the_staging_ring(ts):
     ctx.close()
 
 
+@pytest.mark.parametrize("t", PIPE_TYPES)
+def test_keys_order_pipeline_matches_oracle(ts, t):
+    """sort_by_key's order() through the pipeline: chunk orders merged by the
+    keys they point to. Few distinct keys make every merge decide ties, where
+    only a stable merge gives the crate's permutation."""
+    ctx = ts.Context(0)
+    rng = np.random.default_rng(abs(hash(("order", t))) % 2**32)
+    for chunks in (2, 8):
+        ctx.transfer_pipeline(chunks, 0)
+        for n in (chunks * 256, chunks * 256 + 1, 100_003, (1 << 20) + 17):
+            for shape in ("random", "few", "asc", "desc", "const"):
+                a = gen(t, n, shape, rng)
+                got = ts.keys_order(a, ctx)
+                assert got.tobytes() == O.sort_by_key_order(a).tobytes(), (t, chunks, n, shape)
+    ctx.close()
+
+
+def test_keys_order_pipeline_pinned_and_large(ts):
+    """Pinned keys and order (straight DMAs), and a pageable 2^25-key u64
+    slice whose keys and order wrap the staging ring."""
+    import torch
+
+    ctx = ts.Context(0)
+    rng = np.random.default_rng(13)
+    ctx.transfer_pipeline(16, 0)
+    a = gen("f64", 3_000_017, "few", rng)
+    keys = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(a.dtype)
+    np.copyto(keys, a)
+    out = torch.empty(a.size * 4, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint32)
+    ts.keys_order(keys, ctx, out=out)
+    assert out.tobytes() == O.sort_by_key_order(a).tobytes()
+    ctx.transfer_pipeline(8, 64 << 20)
+    b = gen("u64", (1 << 25) + 999, "random", rng) % np.uint64(1 << 20)
+    assert ts.keys_order(b, ctx).tobytes() == O.sort_by_key_order(b).tobytes()
+    ctx.close()
+
+
 def test_rejects_bad_chunk_counts(ts):
     ctx = ts.Context(0)
     for bad in (0, 3, 12, 128):

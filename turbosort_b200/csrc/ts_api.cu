@@ -147,6 +147,11 @@ static ts_status host_order(ts_ctx* c, const T* keys, size_t n, uint32_t* order)
         order[0] = 0;
         return TS_OK;
     }
+    if constexpr (sizeof(U) > 1) {
+        if (c->transfer_chunks > 1 && n * (sizeof(U) + 4) >= c->transfer_min_bytes &&
+            n >= (size_t)c->transfer_chunks * 256)
+            return pipeline_order<U, XF>(c, (const U*)keys, n, order);
+    }
     ts_status s;
     if ((s = grow(c, c->keys, n * sizeof(U), "keys")) != TS_OK) return s;
     if ((s = grow(c, c->order, n * 4, "order")) != TS_OK) return s;
@@ -237,7 +242,7 @@ void ts_ctx_destroy(ts_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg,
-                      &c->learn, &c->pipe})
+                      &c->learn, &c->pipe, &c->pipe_pos[0], &c->pipe_pos[1]})
         if (b->p) cudaFree(b->p);
     for (auto ev : c->pipe_events) cudaEventDestroy(ev);
     for (auto ev : c->stage_events) cudaEventDestroy(ev);

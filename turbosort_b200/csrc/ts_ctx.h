@@ -39,6 +39,7 @@ struct ts_ctx {
     ts::DevBuf seg;                // segmented sort: plan, work counter, bin lists, offsets
     ts::DevBuf learn;              // learned partition: sample, model, training state, bucket counts
     ts::DevBuf pipe;               // host-slice pipeline: merge split points
+    ts::DevBuf pipe_pos[2];        // host-slice pipeline of sort_by_key: position runs
     uint32_t* d_error = nullptr;   // kernel-reported errors, read and cleared by the host
 
     // segmented sort: the method of each on-chip length bin per key width
@@ -98,6 +99,9 @@ ts_status order_device(ts_ctx* c, const U* d_keys, size_t n, uint32_t* d_order);
 // The host slice h[0, n) sorted with its copies overlapped; returns when done.
 template <typename U, int XF>
 ts_status pipeline_sort(ts_ctx* c, U* h, size_t n);
+// The stable order of the host keys h_keys[0, n) with the copies overlapped.
+template <typename U, int XF>
+ts_status pipeline_order(ts_ctx* c, const U* h_keys, size_t n, uint32_t* h_order);
 
 }  // namespace ts
 

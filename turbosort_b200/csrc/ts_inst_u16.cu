@@ -10,4 +10,6 @@ template ts_status order_device<uint16_t, 0>(ts_ctx*, const uint16_t*, size_t, u
 template ts_status order_device<uint16_t, 1>(ts_ctx*, const uint16_t*, size_t, uint32_t*);
 template ts_status pipeline_sort<uint16_t, 0>(ts_ctx*, uint16_t*, size_t);
 template ts_status pipeline_sort<uint16_t, 1>(ts_ctx*, uint16_t*, size_t);
+template ts_status pipeline_order<uint16_t, 0>(ts_ctx*, const uint16_t*, size_t, uint32_t*);
+template ts_status pipeline_order<uint16_t, 1>(ts_ctx*, const uint16_t*, size_t, uint32_t*);
 }  // namespace ts

@@ -13,4 +13,7 @@ template ts_status order_device<uint64_t, 2>(ts_ctx*, const uint64_t*, size_t, u
 template ts_status pipeline_sort<uint64_t, 0>(ts_ctx*, uint64_t*, size_t);
 template ts_status pipeline_sort<uint64_t, 1>(ts_ctx*, uint64_t*, size_t);
 template ts_status pipeline_sort<uint64_t, 2>(ts_ctx*, uint64_t*, size_t);
+template ts_status pipeline_order<uint64_t, 0>(ts_ctx*, const uint64_t*, size_t, uint32_t*);
+template ts_status pipeline_order<uint64_t, 1>(ts_ctx*, const uint64_t*, size_t, uint32_t*);
+template ts_status pipeline_order<uint64_t, 2>(ts_ctx*, const uint64_t*, size_t, uint32_t*);
 }  // namespace ts

@@ -73,24 +73,22 @@ inline ts_status pipe_resources(ts_ctx* c, size_t events) {
     return TS_OK;
 }
 
-// Merge sorted runs a and b into out on the context's stream. When `sliced`,
-// the merge runs in PIPE_SLICES output slices; slice p ends at slice_end[p]
-// and its completion is recorded in slice_ev[p].
-template <typename U, int XF>
-ts_status enqueue_merge(ts_ctx* c, const U* a, size_t na, const U* b, size_t nb, U* out, bool sliced,
-                        cudaEvent_t* slice_ev, size_t* slice_end) {
-    const size_t total = na + nb;
+// One merge of `total` outputs on the context's stream: splits(grid,
+// tiles) launches the split search, tiles(grid, t0, t1) a range of output
+// tiles. When `sliced` the tiles go in PIPE_SLICES output slices; slice p
+// ends at output slice_end[p] and its completion is recorded in slice_ev[p].
+template <typename Splits, typename Tiles>
+ts_status enqueue_merge_launches(ts_ctx* c, size_t total, bool sliced, cudaEvent_t* slice_ev, size_t* slice_end,
+                                 Splits splits, Tiles tiles_fn) {
     const size_t tiles = (total + MERGE_TILE - 1) / MERGE_TILE;
-    size_t* split = (size_t*)c->pipe.p;
     const int sg = (int)std::min<size_t>((tiles + 1 + 255) / 256, (size_t)c->sm_count * 8);
-    k_merge_splits<U, XF><<<std::max(sg, 1), 256, 0, c->stream>>>(a, na, b, nb, tiles, split);
+    splits(std::max(sg, 1), tiles);
     ++c->launches;
     const int parts = sliced ? PIPE_SLICES : 1;
     for (int p = 0; p < parts; ++p) {
         const size_t t0 = tiles * p / parts, t1 = tiles * (p + 1) / parts;
         if (t1 > t0) {
-            const int grid = (int)std::min<size_t>(t1 - t0, (size_t)c->sm_count * 8);
-            k_merge_tiles<U, XF><<<grid, MERGE_THREADS, 0, c->stream>>>(a, na, b, nb, out, split, t0, t1);
+            tiles_fn((int)std::min<size_t>(t1 - t0, (size_t)c->sm_count * 8), t0, t1);
             ++c->launches;
         }
         if (sliced) {
@@ -102,131 +100,108 @@ ts_status enqueue_merge(ts_ctx* c, const U* a, size_t na, const U* b, size_t nb,
     return TS_OK;
 }
 
+// Merge sorted key runs a and b into out.
 template <typename U, int XF>
-ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
-    const int C = c->transfer_chunks;
-    ts_status s;
-    if ((s = grow(c, c->keys, n * sizeof(U), "keys")) != TS_OK) return s;
-    if ((s = grow(c, c->alt, n * sizeof(U), "scratch keys")) != TS_OK) return s;
-    if ((s = grow(c, c->pipe, ((n + MERGE_TILE - 1) / MERGE_TILE + 1) * sizeof(size_t), "merge splits")) != TS_OK)
-        return s;
-    if ((s = pipe_resources(c, (size_t)C + PIPE_SLICES + 2)) != TS_OK) return s;
-    cudaPointerAttributes pa{};
-    bool pageable = cudaPointerGetAttributes(&pa, h) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered;
-    cudaGetLastError();
-    if (pageable && !stage_resources(c)) pageable = false;
-    char* stage = (char*)c->stage;
+ts_status enqueue_merge(ts_ctx* c, const U* a, size_t na, const U* b, size_t nb, U* out, bool sliced,
+                        cudaEvent_t* slice_ev, size_t* slice_end) {
+    size_t* split = (size_t*)c->pipe.p;
+    return enqueue_merge_launches(
+        c, na + nb, sliced, slice_ev, slice_end,
+        [&](int g, size_t tiles) { k_merge_splits<U, XF><<<g, 256, 0, c->stream>>>(a, na, b, nb, tiles, split); },
+        [&](int g, size_t t0, size_t t1) {
+            k_merge_tiles<U, XF><<<g, MERGE_THREADS, 0, c->stream>>>(a, na, b, nb, out, split, t0, t1);
+        });
+}
+
+// Merge position runs a (+ a_base) and b (+ b_base) of `keys` into out.
+template <typename U, int XF>
+ts_status enqueue_merge_pos(ts_ctx* c, const U* keys, const uint32_t* a, size_t na, uint32_t a_base,
+                            const uint32_t* b, size_t nb, uint32_t b_base, uint32_t* out, bool sliced,
+                            cudaEvent_t* slice_ev, size_t* slice_end) {
+    size_t* split = (size_t*)c->pipe.p;
+    return enqueue_merge_launches(
+        c, na + nb, sliced, slice_ev, slice_end,
+        [&](int g, size_t tiles) {
+            k_merge_pos_splits<U, XF><<<g, 256, 0, c->stream>>>(keys, a, na, a_base, b, nb, b_base, tiles, split);
+        },
+        [&](int g, size_t t0, size_t t1) {
+            k_merge_pos_tiles<U, XF><<<g, MERGE_THREADS, 0, c->stream>>>(keys, a, na, a_base, b, nb, b_base, out,
+                                                                         split, t0, t1);
+        });
+}
+
+// The copies of one pipelined call, on the copy stream: straight DMAs for a
+// pinned (or registered) host slice, the staging slots for a pageable one.
+struct Transfer {
+    ts_ctx* c;
+    bool pageable = false;
     int slot = 0;
-    // staged copy in of h[b, e): each slot waits for its previous DMA, is
-    // filled by the copy threads, then goes to the device
-    auto staged_in = [&](U* dst, const U* src, size_t count) -> ts_status {
-        const size_t per = STAGE_SLOT_BYTES / sizeof(U);
-        for (size_t q = 0; q < count; q += per) {
-            const size_t m = std::min(per, count - q);
+
+    Transfer(ts_ctx* ctx, const void* host) : c(ctx) {
+        cudaPointerAttributes pa{};
+        pageable = cudaPointerGetAttributes(&pa, host) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered;
+        cudaGetLastError();
+        if (pageable && !stage_resources(c)) pageable = false;
+    }
+
+    // host[0, bytes) to dev: each slot waits for its previous DMA, is filled
+    // by the copy threads, then goes to the device
+    ts_status in(void* dev, const void* host, size_t bytes) {
+        if (bytes == 0) return TS_OK;
+        if (!pageable) {
+            TS_CUDA(c, cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, c->copy_stream));
+            return TS_OK;
+        }
+        for (size_t q = 0; q < bytes; q += STAGE_SLOT_BYTES) {
+            const size_t m = std::min(STAGE_SLOT_BYTES, bytes - q);
             TS_CUDA(c, cudaEventSynchronize(c->stage_events[slot]));
-            char* buf = stage + (size_t)slot * STAGE_SLOT_BYTES;
-            c->copy_pool->copy(buf, src + q, m * sizeof(U));
-            TS_CUDA(c, cudaMemcpyAsync(dst + q, buf, m * sizeof(U), cudaMemcpyHostToDevice, c->copy_stream));
+            char* buf = (char*)c->stage + (size_t)slot * STAGE_SLOT_BYTES;
+            c->copy_pool->copy(buf, (const char*)host + q, m);
+            TS_CUDA(c, cudaMemcpyAsync((char*)dev + q, buf, m, cudaMemcpyHostToDevice, c->copy_stream));
             TS_CUDA(c, cudaEventRecord(c->stage_events[slot], c->copy_stream));
             slot = (slot + 1) % STAGE_SLOTS;
         }
         return TS_OK;
-    };
-    U* X = (U*)c->keys.p;
-    U* Y = (U*)c->alt.p;
-    const size_t chunk = ((n + C - 1) / C + 255) / 256 * 256;  // chunk starts 256 keys apart: 16-byte aligned
-    auto lo = [&](int i) { return std::min(n, (size_t)i * chunk); };
-    cudaEvent_t* in_ev = c->pipe_events.data();         // [C] chunk i is on the device
-    cudaEvent_t* out_ev = in_ev + C;                    // [PIPE_SLICES] output slice p is merged
-    cudaEvent_t ready_ev = in_ev[C + PIPE_SLICES];      // the context's stream reached this call
-    cudaEvent_t done_ev = in_ev[C + PIPE_SLICES + 1];   // the last copy out ended
-
-    // the copies start behind whatever the context's stream already holds
-    TS_CUDA(c, cudaEventRecord(ready_ev, c->stream));
-    TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ready_ev, 0));
-    auto copy_in = [&](int i) -> ts_status {
-        if (i >= C) return TS_OK;
-        const size_t b = lo(i), e = lo(i + 1);
-        if (e > b) {
-            if (pageable) {
-                ts_status st = staged_in(X + b, h + b, e - b);
-                if (st != TS_OK) return st;
-            } else {
-                TS_CUDA(c, cudaMemcpyAsync(X + b, h + b, (e - b) * sizeof(U), cudaMemcpyHostToDevice, c->copy_stream));
-            }
-        }
-        TS_CUDA(c, cudaEventRecord(in_ev[i], c->copy_stream));
-        return TS_OK;
-    };
-    mark(c, "pipeline");
-    if ((s = copy_in(0)) != TS_OK) return s;
-    if ((s = copy_in(1)) != TS_OK) return s;
-
-    struct Run {
-        size_t b, e;
-        int level;
-    };
-    std::vector<Run> runs;
-    size_t slice_end[PIPE_SLICES] = {};
-    U* final_buf = X;
-    for (int i = 0; i < C; ++i) {
-        TS_CUDA(c, cudaStreamWaitEvent(c->stream, in_ev[i], 0));
-        const size_t b = lo(i), e = lo(i + 1);
-        if ((s = sort_keys_device<U, XF>(c, X + b, e - b, Y + b)) != TS_OK) return s;
-        runs.push_back({b, e, 0});
-        while (runs.size() >= 2 && runs[runs.size() - 1].level == runs[runs.size() - 2].level) {
-            const Run r2 = runs.back();
-            runs.pop_back();
-            const Run r1 = runs.back();
-            runs.pop_back();
-            const int L = r1.level;
-            U* src = (L & 1) ? Y : X;
-            U* dst = (L & 1) ? X : Y;
-            const bool last = i == C - 1 && runs.empty();
-            mark(c, "merge");
-            if ((s = enqueue_merge<U, XF>(c, src + r1.b, r1.e - r1.b, src + r2.b, r2.e - r2.b, dst + r1.b, last, out_ev,
-                                          slice_end)) != TS_OK)
-                return s;
-            runs.push_back({r1.b, r2.e, L + 1});
-            if (last) final_buf = dst;
-        }
-        if ((s = copy_in(i + 2)) != TS_OK) return s;
     }
-    mark(c, "end");
-    // the sorted slice goes back one merged output slice at a time
-    if (!pageable) {
-        size_t from = 0;
-        for (int p = 0; p < PIPE_SLICES; ++p) {
-            TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, out_ev[p], 0));
-            if (slice_end[p] > from)
-                TS_CUDA(c, cudaMemcpyAsync(h + from, final_buf + from, (slice_end[p] - from) * sizeof(U),
-                                           cudaMemcpyDeviceToHost, c->copy_stream));
-            from = std::max(from, slice_end[p]);
+
+    // dev to host, slice by slice: slice p (bytes up to end[p]) once
+    // slice_ev[p] has happened on the context's stream. Pageable: pieces of
+    // at most one slot, none across a slice end; the DMA of piece
+    // k + STAGE_SLOTS - 1 is queued before the threads empty piece k.
+    ts_status out(void* host, const void* dev, const size_t* end, cudaEvent_t* slice_ev, int slices) {
+        if (!pageable) {
+            size_t from = 0;
+            for (int p = 0; p < slices; ++p) {
+                TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, slice_ev[p], 0));
+                if (end[p] > from)
+                    TS_CUDA(c, cudaMemcpyAsync((char*)host + from, (const char*)dev + from, end[p] - from,
+                                               cudaMemcpyDeviceToHost, c->copy_stream));
+                from = std::max(from, end[p]);
+            }
+            return TS_OK;
         }
-    } else {
-        // pieces of at most one slot, none across a slice end; the DMA of
-        // piece k + STAGE_SLOTS - 1 is queued before the threads empty piece k
         struct Piece {
             size_t b, e;
             int slice;
         };
         std::vector<Piece> pieces;
-        const size_t per = STAGE_SLOT_BYTES / sizeof(U);
         size_t from = 0;
-        for (int p = 0; p < PIPE_SLICES; ++p) {
-            for (size_t q = from; q < slice_end[p]; q += per) pieces.push_back({q, std::min(slice_end[p], q + per), p});
-            from = std::max(from, slice_end[p]);
+        for (int p = 0; p < slices; ++p) {
+            for (size_t q = from; q < end[p]; q += STAGE_SLOT_BYTES)
+                pieces.push_back({q, std::min(end[p], q + STAGE_SLOT_BYTES), p});
+            from = std::max(from, end[p]);
         }
         int waited = -1;  // the last slice the copy stream waits for
         auto issue = [&](size_t k) -> ts_status {
             const Piece& pc = pieces[k];
-            for (; waited < pc.slice; ++waited) TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, out_ev[waited + 1], 0));
+            for (; waited < pc.slice; ++waited) TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, slice_ev[waited + 1], 0));
             const int sl = (int)(k % STAGE_SLOTS);
-            TS_CUDA(c, cudaMemcpyAsync(stage + (size_t)sl * STAGE_SLOT_BYTES, final_buf + pc.b, (pc.e - pc.b) * sizeof(U),
-                                       cudaMemcpyDeviceToHost, c->copy_stream));
+            TS_CUDA(c, cudaMemcpyAsync((char*)c->stage + (size_t)sl * STAGE_SLOT_BYTES, (const char*)dev + pc.b,
+                                       pc.e - pc.b, cudaMemcpyDeviceToHost, c->copy_stream));
             TS_CUDA(c, cudaEventRecord(c->stage_events[sl], c->copy_stream));
             return TS_OK;
         };
+        ts_status s;
         for (size_t k = 0; k + 1 < (size_t)STAGE_SLOTS && k < pieces.size(); ++k)
             if ((s = issue(k)) != TS_OK) return s;
         for (size_t k = 0; k < pieces.size(); ++k) {
@@ -234,27 +209,166 @@ ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
                 if ((s = issue(k + STAGE_SLOTS - 1)) != TS_OK) return s;
             const int sl = (int)(k % STAGE_SLOTS);
             TS_CUDA(c, cudaEventSynchronize(c->stage_events[sl]));
-            c->copy_pool->copy(h + pieces[k].b, stage + (size_t)sl * STAGE_SLOT_BYTES,
-                               (pieces[k].e - pieces[k].b) * sizeof(U));
+            c->copy_pool->copy((char*)host + pieces[k].b, (const char*)c->stage + (size_t)sl * STAGE_SLOT_BYTES,
+                               pieces[k].e - pieces[k].b);
         }
+        return TS_OK;
     }
-    TS_CUDA(c, cudaEventRecord(done_ev, c->copy_stream));
-    TS_CUDA(c, cudaStreamWaitEvent(c->stream, done_ev, 0));
+};
+
+// The chunks, the merge tree over their sorted runs, and the copies of one
+// pipelined call. sort_chunk(i, b, e) enqueues chunk i's sort (into its
+// level-0 run); merge(L, r1, r2, last) enqueues the merge of two level-L
+// runs. The copy in of chunk i + 2 is issued after chunk i's sort, so a
+// pageable slice, whose staged copies hold this thread, overlaps the work
+// already queued.
+template <typename CopyIn, typename SortChunk, typename Merge>
+ts_status run_pipeline(ts_ctx* c, size_t n, CopyIn copy_chunk, SortChunk sort_chunk, Merge merge) {
+    const int C = c->transfer_chunks;
+    const size_t chunk = ((n + C - 1) / C + 255) / 256 * 256;  // chunk starts 256 elements apart: 16-byte aligned
+    auto lo = [&](int i) { return std::min(n, (size_t)i * chunk); };
+    cudaEvent_t* in_ev = c->pipe_events.data();  // [C] chunk i is on the device
+    ts_status s;
+    // the copies start behind whatever the context's stream already holds
+    cudaEvent_t ready_ev = in_ev[C + PIPE_SLICES];
+    TS_CUDA(c, cudaEventRecord(ready_ev, c->stream));
+    TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ready_ev, 0));
+    auto copy_in = [&](int i) -> ts_status {
+        if (i >= C) return TS_OK;
+        ts_status st = copy_chunk(lo(i), lo(i + 1));
+        if (st != TS_OK) return st;
+        TS_CUDA(c, cudaEventRecord(in_ev[i], c->copy_stream));
+        return TS_OK;
+    };
+    mark(c, "pipeline");
+    if ((s = copy_in(0)) != TS_OK) return s;
+    if ((s = copy_in(1)) != TS_OK) return s;
+    struct Run {
+        size_t b, e;
+        int level;
+    };
+    std::vector<Run> runs;
+    for (int i = 0; i < C; ++i) {
+        TS_CUDA(c, cudaStreamWaitEvent(c->stream, in_ev[i], 0));
+        if ((s = sort_chunk(lo(i), lo(i + 1))) != TS_OK) return s;
+        runs.push_back({lo(i), lo(i + 1), 0});
+        while (runs.size() >= 2 && runs[runs.size() - 1].level == runs[runs.size() - 2].level) {
+            const Run r2 = runs.back();
+            runs.pop_back();
+            const Run r1 = runs.back();
+            runs.pop_back();
+            mark(c, "merge");
+            if ((s = merge(r1.level, r1.b, r1.e, r2.e, i == C - 1 && runs.empty())) != TS_OK) return s;
+            runs.push_back({r1.b, r2.e, r1.level + 1});
+        }
+        if ((s = copy_in(i + 2)) != TS_OK) return s;
+    }
+    mark(c, "end");
     return TS_OK;
 }
 
-// Sort the host slice h[0, n) with the copies overlapped (c->transfer_chunks
-// a power of two, at least 2). Returns once the sorted keys are back in h.
-template <typename U, int XF>
-ts_status pipeline_sort(ts_ctx* c, U* h, size_t n) {
-    ts_status s = pipeline_body<U, XF>(c, h, n);
+// the events a pipelined call records: [C] chunks in, [PIPE_SLICES] output
+// slices merged, then "stream reached the call" and "copies out done"
+inline cudaEvent_t* slice_events(ts_ctx* c) { return c->pipe_events.data() + c->transfer_chunks; }
+inline cudaEvent_t done_event(ts_ctx* c) { return c->pipe_events[c->transfer_chunks + PIPE_SLICES + 1]; }
+
+// whatever failed, nothing may still copy into or out of the caller's slices
+inline ts_status pipeline_end(ts_ctx* c, ts_status s) {
     if (s != TS_OK) {
-        // nothing may still be copying into or out of the caller's slice
         if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
         cudaStreamSynchronize(c->stream);
         return s;
     }
     return finish(c);
+}
+
+// Sort the host slice h[0, n) with the copies overlapped (c->transfer_chunks
+// a power of two, at least 2). Returns once the sorted keys are back in h.
+template <typename U, int XF>
+ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
+    ts_status s;
+    if ((s = grow(c, c->keys, n * sizeof(U), "keys")) != TS_OK) return s;
+    if ((s = grow(c, c->alt, n * sizeof(U), "scratch keys")) != TS_OK) return s;
+    if ((s = grow(c, c->pipe, ((n + MERGE_TILE - 1) / MERGE_TILE + 1) * sizeof(size_t), "merge splits")) != TS_OK)
+        return s;
+    if ((s = pipe_resources(c, (size_t)c->transfer_chunks + PIPE_SLICES + 2)) != TS_OK) return s;
+    Transfer T(c, h);
+    U* X = (U*)c->keys.p;  // chunks arrive here; even merge levels
+    U* Y = (U*)c->alt.p;   // odd merge levels; a chunk sort's scratch
+    size_t slice_end[PIPE_SLICES] = {};
+    U* final_buf = X;
+    s = run_pipeline(
+        c, n, [&](size_t b, size_t e) { return T.in(X + b, h + b, (e - b) * sizeof(U)); },
+        [&](size_t b, size_t e) { return sort_keys_device<U, XF>(c, X + b, e - b, Y + b); },
+        [&](int L, size_t b, size_t m, size_t e, bool last) {
+            U* src = (L & 1) ? Y : X;
+            U* dst = (L & 1) ? X : Y;
+            if (last) final_buf = dst;
+            return enqueue_merge<U, XF>(c, src + b, m - b, src + m, e - m, dst + b, last, slice_events(c), slice_end);
+        });
+    if (s != TS_OK) return s;
+    size_t end_bytes[PIPE_SLICES];
+    for (int p = 0; p < PIPE_SLICES; ++p) end_bytes[p] = slice_end[p] * sizeof(U);
+    if ((s = T.out(h, final_buf, end_bytes, slice_events(c), PIPE_SLICES)) != TS_OK) return s;
+    TS_CUDA(c, cudaEventRecord(done_event(c), c->copy_stream));
+    TS_CUDA(c, cudaStreamWaitEvent(c->stream, done_event(c), 0));
+    return TS_OK;
+}
+
+template <typename U, int XF>
+ts_status pipeline_sort(ts_ctx* c, U* h, size_t n) {
+    return pipeline_end(c, pipeline_body<U, XF>(c, h, n));
+}
+
+// The stable order of the host keys h_keys[0, n) (sort_by_key's order(),
+// src/by_key.rs:175-233) with the copies overlapped: each chunk's keys are
+// ordered by the device's stable LSD (positions within the chunk), and the
+// position runs are merged by the keys they point to, which stay where they
+// arrived. Returns once order[0, n) is back on the host.
+template <typename U, int XF>
+ts_status pipeline_order_body(ts_ctx* c, const U* h_keys, size_t n, uint32_t* h_order) {
+    ts_status s;
+    if ((s = grow(c, c->keys, n * sizeof(U), "keys")) != TS_OK) return s;
+    if ((s = grow(c, c->pipe_pos[0], n * 4, "positions")) != TS_OK) return s;
+    if ((s = grow(c, c->pipe_pos[1], n * 4, "positions")) != TS_OK) return s;
+    if ((s = grow(c, c->pipe, ((n + MERGE_TILE - 1) / MERGE_TILE + 1) * sizeof(size_t), "merge splits")) != TS_OK)
+        return s;
+    if ((s = pipe_resources(c, (size_t)c->transfer_chunks + PIPE_SLICES + 2)) != TS_OK) return s;
+    Transfer Tin(c, h_keys), Tout(c, h_order);  // the two share the staging slots, in stream order
+    U* X = (U*)c->keys.p;
+    uint32_t* P[2] = {(uint32_t*)c->pipe_pos[0].p, (uint32_t*)c->pipe_pos[1].p};
+    size_t slice_end[PIPE_SLICES] = {};
+    uint32_t* final_buf = P[0];
+    s = run_pipeline(
+        c, n, [&](size_t b, size_t e) { return Tin.in(X + b, h_keys + b, (e - b) * sizeof(U)); },
+        [&](size_t b, size_t e) -> ts_status {
+            if (e - b == 1) {
+                TS_CUDA(c, cudaMemsetAsync(P[0] + b, 0, 4, c->stream));
+                return TS_OK;
+            }
+            return order_device<U, XF>(c, X + b, e - b, P[0] + b);
+        },
+        [&](int L, size_t b, size_t m, size_t e, bool last) {
+            uint32_t* src = P[L & 1];
+            uint32_t* dst = P[(L + 1) & 1];
+            if (last) final_buf = dst;
+            // level-0 runs hold positions within their chunk
+            const uint32_t ab = L == 0 ? (uint32_t)b : 0u, bb = L == 0 ? (uint32_t)m : 0u;
+            return enqueue_merge_pos<U, XF>(c, X, src + b, m - b, ab, src + m, e - m, bb, dst + b, last,
+                                            slice_events(c), slice_end);
+        });
+    if (s != TS_OK) return s;
+    size_t end_bytes[PIPE_SLICES];
+    for (int p = 0; p < PIPE_SLICES; ++p) end_bytes[p] = slice_end[p] * 4;
+    if ((s = Tout.out(h_order, final_buf, end_bytes, slice_events(c), PIPE_SLICES)) != TS_OK) return s;
+    TS_CUDA(c, cudaEventRecord(done_event(c), c->copy_stream));
+    TS_CUDA(c, cudaStreamWaitEvent(c->stream, done_event(c), 0));
+    return TS_OK;
+}
+
+template <typename U, int XF>
+ts_status pipeline_order(ts_ctx* c, const U* h_keys, size_t n, uint32_t* h_order) {
+    return pipeline_end(c, pipeline_order_body<U, XF>(c, h_keys, n, h_order));
 }
 
 }  // namespace ts
