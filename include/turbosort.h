@@ -66,7 +66,9 @@ size_t ts_ctx_capacity(const ts_ctx *ctx, size_t key_bytes, int with_order);
  * two, 1 to 64) on a second stream: each piece is sorted (or ordered) while
  * the next one is in flight, the pieces' results are merged pairwise on the
  * device, and the last merge's output is copied back slice by slice while
- * the rest is merged. A pageable host slice goes through pinned staging
+ * the rest is merged. Host ts_apply_order copies back its gather slice by
+ * slice, and host ts_sort_segments_<T> sorts groups of whole segments as
+ * they arrive and copies each back at once. A pageable host slice goes through pinned staging
  * slots of the context, filled and emptied by host threads. chunks = 1
  * copies in, sorts and copies out. The output is the same either way.
  * Default: 8 chunks from 64 MiB. */

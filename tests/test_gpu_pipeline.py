@@ -155,6 +155,74 @@ def test_keys_order_pipeline_pinned_and_large(ts):
     ctx.close()
 
 
+def test_apply_order_pipeline_matches_oracle(ts):
+    """Host apply_order with the copies overlapped (the gather in output
+    slices, each copied back while the next is gathered), for element sizes
+    that take every gather word width, pageable and pinned."""
+    import torch
+
+    ctx = ts.Context(0)
+    ctx.transfer_pipeline(8, 0)
+    rng = np.random.default_rng(17)
+    for n in (8 * 256, 100_003, (1 << 20) + 5):
+        order = rng.permutation(n).astype(np.uint32)
+        for elem in (1, 3, 4, 8, 12, 16, 24):
+            data = rng.integers(0, 256, size=(n, elem), dtype=np.uint8)
+            want = O.apply_order(data, order)
+            got = data.copy()
+            ts.apply_order(got, order, ctx)
+            assert got.tobytes() == want.tobytes(), (n, elem)
+        pinned = torch.empty(n * 16, dtype=torch.uint8, pin_memory=True).numpy().reshape(n, 16)
+        data = rng.integers(0, 256, size=(n, 16), dtype=np.uint8)
+        np.copyto(pinned, data)
+        ts.apply_order(pinned, order, ctx)
+        assert pinned.tobytes() == O.apply_order(data, order).tobytes(), n
+    ctx.close()
+
+
+def _segments_case(rng, t, count, huge):
+    lengths = rng.integers(0, 3000, size=count)
+    lengths[rng.integers(0, count, size=count // 10)] = 0
+    if huge:
+        lengths[count // 3] = (1 << 22) + 5  # above the host path's limit: the device-wide sort
+    offs = np.zeros(count + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum(lengths) + 77  # keys before the first segment and after the last stay put
+    offs[0] = 77
+    n = int(offs[-1]) + 123
+    return gen(t, n, "random", rng), offs
+
+
+def _segments_want(a, offs):
+    want = a.copy()
+    for i in range(offs.size - 1):
+        lo, hi = int(offs[i]), int(offs[i + 1])
+        if hi - lo > 1:
+            want[lo:hi] = O.sort(a[lo:hi])
+    return want
+
+
+@pytest.mark.parametrize("t", ["u32", "f32", "u64", "i16"])
+def test_segments_pipeline_matches_oracle(ts, t):
+    """Host segmented sort in groups of whole segments, each sorted while
+    later groups cross and copied back at once (pinned) or after (pageable)."""
+    import torch
+
+    ctx = ts.Context(0)
+    rng = np.random.default_rng(abs(hash(("seg", t))) % 2**32)
+    for chunks, count, huge in ((2, 50, False), (8, 1500, True), (64, 700, False)):
+        ctx.transfer_pipeline(chunks, 0)
+        a, offs = _segments_case(rng, t, count, huge)
+        want = _segments_want(a, offs)
+        got = a.copy()
+        ts.sort_segments(got, offs, ctx)
+        assert got.tobytes() == want.tobytes(), (t, chunks, count)
+        pinned = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(a.dtype)
+        np.copyto(pinned, a)
+        ts.sort_segments(pinned, offs, ctx)
+        assert pinned.tobytes() == want.tobytes(), (t, chunks, count, "pinned")
+    ctx.close()
+
+
 def test_rejects_bad_chunk_counts(ts):
     ctx = ts.Context(0)
     for bad in (0, 3, 12, 128):

@@ -10,7 +10,7 @@
 
 #include "ts_ctx.h"
 #include "ts_gather.cuh"
-#include "ts_staging.h"
+#include "ts_transfer.h"
 
 namespace ts {
 
@@ -184,25 +184,67 @@ static ts_status dev_order(ts_ctx* c, const U* d, size_t n, uint32_t* order) {
     return order_device<U, XF>(c, d, n, order);
 }
 
-static ts_status gather_dev(ts_ctx* c, const void* in, void* out, const uint32_t* order, size_t n, size_t elem) {
-    const size_t bytes = n * elem;
+// out[i] = in[order[i]] for i < n, elements of `elem` bytes; order[i] < n_src
+static ts_status gather_dev(ts_ctx* c, const void* in, void* out, const uint32_t* order, size_t n, size_t elem,
+                            size_t n_src) {
     const int grid = c->sm_count * 8;
     if (elem % 16 == 0 && ((uintptr_t)in & 15) == 0 && ((uintptr_t)out & 15) == 0) {
-        k_gather<uint4><<<grid, 256, 0, c->stream>>>((const uint4*)in, (uint4*)out, order, n, (uint32_t)(elem / 16),
-                                                     c->d_error);
+        k_gather<uint4><<<grid, 256, 0, c->stream>>>((const uint4*)in, (uint4*)out, order, n, n_src,
+                                                     (uint32_t)(elem / 16), c->d_error);
     } else if (elem % 8 == 0 && ((uintptr_t)in & 7) == 0 && ((uintptr_t)out & 7) == 0) {
-        k_gather<uint2><<<grid, 256, 0, c->stream>>>((const uint2*)in, (uint2*)out, order, n, (uint32_t)(elem / 8),
-                                                     c->d_error);
+        k_gather<uint2><<<grid, 256, 0, c->stream>>>((const uint2*)in, (uint2*)out, order, n, n_src,
+                                                     (uint32_t)(elem / 8), c->d_error);
     } else if (elem % 4 == 0 && ((uintptr_t)in & 3) == 0 && ((uintptr_t)out & 3) == 0) {
-        k_gather<uint32_t><<<grid, 256, 0, c->stream>>>((const uint32_t*)in, (uint32_t*)out, order, n,
+        k_gather<uint32_t><<<grid, 256, 0, c->stream>>>((const uint32_t*)in, (uint32_t*)out, order, n, n_src,
                                                         (uint32_t)(elem / 4), c->d_error);
     } else {
-        k_gather<uint8_t><<<grid, 256, 0, c->stream>>>((const uint8_t*)in, (uint8_t*)out, order, n, (uint32_t)elem,
-                                                       c->d_error);
+        k_gather<uint8_t><<<grid, 256, 0, c->stream>>>((const uint8_t*)in, (uint8_t*)out, order, n, n_src,
+                                                       (uint32_t)elem, c->d_error);
     }
-    (void)bytes;
     ++c->launches;
     TS_CUDA(c, cudaGetLastError());
+    return TS_OK;
+}
+
+// Host apply_order with its copies overlapped: the order and the elements
+// cross on the copy stream (through the staging slots when pageable), the
+// gather runs in PIPE_SLICES output slices, and each slice goes back while
+// the next is gathered.
+static ts_status pipeline_apply_order(ts_ctx* c, void* data, size_t n, size_t elem, const uint32_t* order) {
+    const size_t bytes = n * elem;
+    const size_t half = (bytes + 255) / 256 * 256;
+    ts_status s;
+    if ((s = grow(c, c->gather, 2 * half, "apply_order staging")) != TS_OK) return s;
+    if ((s = grow(c, c->order, n * 4, "order")) != TS_OK) return s;
+    if ((s = pipe_resources(c, (size_t)c->transfer_chunks + PIPE_SLICES + 2)) != TS_OK) return s;
+    char* a = (char*)c->gather.p;
+    char* b = a + half;
+    uint32_t* d_order = (uint32_t*)c->order.p;
+    cudaEvent_t* ev = c->pipe_events.data();
+    Transfer to(c, order), td(c, data);
+    mark(c, "h2d");
+    TS_CUDA(c, cudaEventRecord(ev[0], c->stream));
+    TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ev[0], 0));
+    if ((s = to.in(d_order, order, n * 4)) != TS_OK) return s;
+    td.slot = to.slot;
+    if ((s = td.in(a, data, bytes)) != TS_OK) return s;
+    TS_CUDA(c, cudaEventRecord(ev[1], c->copy_stream));
+    TS_CUDA(c, cudaStreamWaitEvent(c->stream, ev[1], 0));
+    mark(c, "gather");
+    size_t end[PIPE_SLICES];
+    cudaEvent_t* slice_ev = slice_events(c);
+    for (int p = 0; p < PIPE_SLICES; ++p) {
+        // slice starts 256 elements apart keep every slice's output aligned
+        const size_t lo = p == 0 ? 0 : std::min(n, n * p / PIPE_SLICES / 256 * 256);
+        const size_t hi = p + 1 == PIPE_SLICES ? n : std::min(n, n * (p + 1) / PIPE_SLICES / 256 * 256);
+        if (hi > lo && (s = gather_dev(c, a, b + lo * elem, d_order + lo, hi - lo, elem, n)) != TS_OK) return s;
+        end[p] = hi * elem;
+        TS_CUDA(c, cudaEventRecord(slice_ev[p], c->stream));
+    }
+    mark(c, "end");
+    if ((s = td.out(data, b, end, slice_ev, PIPE_SLICES)) != TS_OK) return s;
+    TS_CUDA(c, cudaEventRecord(done_event(c), c->copy_stream));
+    TS_CUDA(c, cudaStreamWaitEvent(c->stream, done_event(c), 0));
     return TS_OK;
 }
 
@@ -241,12 +283,14 @@ void ts_ctx_destroy(ts_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    if (c->out_stream) cudaStreamSynchronize(c->out_stream);
     for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg,
                       &c->learn, &c->pipe, &c->pipe_pos[0], &c->pipe_pos[1]})
         if (b->p) cudaFree(b->p);
     for (auto ev : c->pipe_events) cudaEventDestroy(ev);
     for (auto ev : c->stage_events) cudaEventDestroy(ev);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->out_stream) cudaStreamDestroy(c->out_stream);
     if (c->stage) cudaFreeHost(c->stage);
     delete c->copy_pool;
     if (c->seg_graph) cudaGraphExecDestroy(c->seg_graph);
@@ -406,6 +450,8 @@ ts_status ts_apply_order(ts_ctx* c, void* data, size_t n, size_t elem, const uin
     if (n == 0 || elem == 0) return TS_OK;
     if (!data || !order) return fail(c, TS_ERR_INVALID, "null data or order");
     const size_t bytes = n * elem;
+    if (c->transfer_chunks > 1 && bytes + n * 4 >= c->transfer_min_bytes && n >= (size_t)PIPE_SLICES * 256)
+        return pipeline_end(c, pipeline_apply_order(c, data, n, elem, order));
     const size_t half = (bytes + 255) / 256 * 256;
     ts_status s;
     if ((s = grow(c, c->gather, 2 * half, "apply_order staging")) != TS_OK) return s;
@@ -416,7 +462,7 @@ ts_status ts_apply_order(ts_ctx* c, void* data, size_t n, size_t elem, const uin
     TS_CUDA(c, cudaMemcpyAsync(a, data, bytes, cudaMemcpyHostToDevice, c->stream));
     TS_CUDA(c, cudaMemcpyAsync(c->order.p, order, n * 4, cudaMemcpyHostToDevice, c->stream));
     mark(c, "gather");
-    if ((s = gather_dev(c, a, b, (const uint32_t*)c->order.p, n, elem)) != TS_OK) return s;
+    if ((s = gather_dev(c, a, b, (const uint32_t*)c->order.p, n, elem, n)) != TS_OK) return s;
     mark(c, "d2h");
     TS_CUDA(c, cudaMemcpyAsync(data, b, bytes, cudaMemcpyDeviceToHost, c->stream));
     return finish(c);
@@ -433,7 +479,7 @@ ts_status ts_apply_order_dev(ts_ctx* c, void* d_data, size_t n, size_t elem, con
     ts_status s;
     if ((s = grow(c, c->gather, bytes, "apply_order staging")) != TS_OK) return s;
     mark(c, "gather");
-    if ((s = gather_dev(c, d_data, c->gather.p, d_order, n, elem)) != TS_OK) return s;
+    if ((s = gather_dev(c, d_data, c->gather.p, d_order, n, elem, n)) != TS_OK) return s;
     mark(c, "copy");
     TS_CUDA(c, cudaMemcpyAsync(d_data, c->gather.p, bytes, cudaMemcpyDeviceToDevice, c->stream));
     return TS_OK;

@@ -61,6 +61,7 @@ struct ts_ctx {
     int transfer_chunks = 8;
     size_t transfer_min_bytes = (size_t)64 << 20;
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t out_stream = nullptr;     // copies back that overlap copies in
     std::vector<cudaEvent_t> pipe_events;
     // pageable host slices go through pinned staging slots, filled and
     // emptied by the copy pool's threads

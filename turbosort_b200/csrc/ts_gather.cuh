@@ -15,8 +15,8 @@ constexpr int GATHER_ILP = 4;
 
 template <typename W>
 __global__ void __launch_bounds__(256) k_gather(const W* __restrict__ in, W* __restrict__ out,
-                                                const uint32_t* __restrict__ order, size_t n, uint32_t wpe,
-                                                uint32_t* __restrict__ error) {
+                                                const uint32_t* __restrict__ order, size_t n, size_t n_src,
+                                                uint32_t wpe, uint32_t* __restrict__ error) {
     const size_t total = n * wpe;
     const size_t step = (size_t)gridDim.x * blockDim.x * GATHER_ILP;
     for (size_t base = (size_t)blockIdx.x * blockDim.x * GATHER_ILP + threadIdx.x; base < total; base += step) {
@@ -37,13 +37,13 @@ __global__ void __launch_bounds__(256) k_gather(const W* __restrict__ in, W* __r
 #pragma unroll
         for (int e = 0; e < GATHER_ILP; ++e) {
             const size_t g = base + (size_t)e * blockDim.x;
-            if (g < total && src[e] < n) v[e] = in[(size_t)src[e] * wpe + w[e]];
+            if (g < total && src[e] < n_src) v[e] = in[(size_t)src[e] * wpe + w[e]];
         }
 #pragma unroll
         for (int e = 0; e < GATHER_ILP; ++e) {
             const size_t g = base + (size_t)e * blockDim.x;
             if (g >= total) continue;
-            if (src[e] < n) __stcs(out + g, v[e]);
+            if (src[e] < n_src) __stcs(out + g, v[e]);
             else atomicOr(error, ERR_BOUNDS);
         }
     }

@@ -19,12 +19,7 @@
 // copy of chunk i + 2 is issued after the sort of chunk i and every copy out
 // after the last merge.
 //
-// A pageable host slice cannot be a DMA source or target; the driver would
-// copy it through its own pinned buffer on this thread at about a quarter of
-// the PCIe rate. Such a slice goes through the context's pinned staging
-// slots instead: the copy pool's threads fill a slot while the DMA of the
-// previous one runs, and on the way back empty a slot while the next one's
-// DMA runs.
+// Pageable host slices cross through pinned staging slots (ts_transfer.h).
 #pragma once
 
 #include <algorithm>
@@ -32,46 +27,9 @@
 
 #include "ts_engine.cuh"
 #include "ts_merge.cuh"
-#include "ts_staging.h"
+#include "ts_transfer.h"
 
 namespace ts {
-
-constexpr int PIPE_SLICES = 8;                     // output slices of the last merge
-constexpr int STAGE_SLOTS = 4;                     // pinned staging slots for pageable slices
-constexpr size_t STAGE_SLOT_BYTES = (size_t)32 << 20;
-
-// the pinned slots, their events and the copy threads; false if pinned
-// memory cannot be had (the slice then takes the driver's own staging)
-inline bool stage_resources(ts_ctx* c) {
-    if (!c->stage) {
-        if (cudaHostAlloc(&c->stage, STAGE_SLOTS * STAGE_SLOT_BYTES, cudaHostAllocDefault) != cudaSuccess) {
-            cudaGetLastError();
-            c->stage = nullptr;
-            return false;
-        }
-    }
-    while (c->stage_events.size() < (size_t)STAGE_SLOTS) {
-        cudaEvent_t ev;
-        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        c->stage_events.push_back(ev);
-    }
-    if (!c->copy_pool) c->copy_pool = new CopyPool(copy_pool_workers());
-    return true;
-}
-
-// the copy stream and the events a pipelined call uses, made once per context
-inline ts_status pipe_resources(ts_ctx* c, size_t events) {
-    if (!c->copy_stream) TS_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-    while (c->pipe_events.size() < events) {
-        cudaEvent_t ev;
-        TS_CUDA(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        c->pipe_events.push_back(ev);
-    }
-    return TS_OK;
-}
 
 // One merge of `total` outputs on the context's stream: splits(grid,
 // tiles) launches the split search, tiles(grid, t0, t1) a range of output
@@ -130,92 +88,6 @@ ts_status enqueue_merge_pos(ts_ctx* c, const U* keys, const uint32_t* a, size_t 
         });
 }
 
-// The copies of one pipelined call, on the copy stream: straight DMAs for a
-// pinned (or registered) host slice, the staging slots for a pageable one.
-struct Transfer {
-    ts_ctx* c;
-    bool pageable = false;
-    int slot = 0;
-
-    Transfer(ts_ctx* ctx, const void* host) : c(ctx) {
-        cudaPointerAttributes pa{};
-        pageable = cudaPointerGetAttributes(&pa, host) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered;
-        cudaGetLastError();
-        if (pageable && !stage_resources(c)) pageable = false;
-    }
-
-    // host[0, bytes) to dev: each slot waits for its previous DMA, is filled
-    // by the copy threads, then goes to the device
-    ts_status in(void* dev, const void* host, size_t bytes) {
-        if (bytes == 0) return TS_OK;
-        if (!pageable) {
-            TS_CUDA(c, cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, c->copy_stream));
-            return TS_OK;
-        }
-        for (size_t q = 0; q < bytes; q += STAGE_SLOT_BYTES) {
-            const size_t m = std::min(STAGE_SLOT_BYTES, bytes - q);
-            TS_CUDA(c, cudaEventSynchronize(c->stage_events[slot]));
-            char* buf = (char*)c->stage + (size_t)slot * STAGE_SLOT_BYTES;
-            c->copy_pool->copy(buf, (const char*)host + q, m);
-            TS_CUDA(c, cudaMemcpyAsync((char*)dev + q, buf, m, cudaMemcpyHostToDevice, c->copy_stream));
-            TS_CUDA(c, cudaEventRecord(c->stage_events[slot], c->copy_stream));
-            slot = (slot + 1) % STAGE_SLOTS;
-        }
-        return TS_OK;
-    }
-
-    // dev to host, slice by slice: slice p (bytes up to end[p]) once
-    // slice_ev[p] has happened on the context's stream. Pageable: pieces of
-    // at most one slot, none across a slice end; the DMA of piece
-    // k + STAGE_SLOTS - 1 is queued before the threads empty piece k.
-    ts_status out(void* host, const void* dev, const size_t* end, cudaEvent_t* slice_ev, int slices) {
-        if (!pageable) {
-            size_t from = 0;
-            for (int p = 0; p < slices; ++p) {
-                TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, slice_ev[p], 0));
-                if (end[p] > from)
-                    TS_CUDA(c, cudaMemcpyAsync((char*)host + from, (const char*)dev + from, end[p] - from,
-                                               cudaMemcpyDeviceToHost, c->copy_stream));
-                from = std::max(from, end[p]);
-            }
-            return TS_OK;
-        }
-        struct Piece {
-            size_t b, e;
-            int slice;
-        };
-        std::vector<Piece> pieces;
-        size_t from = 0;
-        for (int p = 0; p < slices; ++p) {
-            for (size_t q = from; q < end[p]; q += STAGE_SLOT_BYTES)
-                pieces.push_back({q, std::min(end[p], q + STAGE_SLOT_BYTES), p});
-            from = std::max(from, end[p]);
-        }
-        int waited = -1;  // the last slice the copy stream waits for
-        auto issue = [&](size_t k) -> ts_status {
-            const Piece& pc = pieces[k];
-            for (; waited < pc.slice; ++waited) TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, slice_ev[waited + 1], 0));
-            const int sl = (int)(k % STAGE_SLOTS);
-            TS_CUDA(c, cudaMemcpyAsync((char*)c->stage + (size_t)sl * STAGE_SLOT_BYTES, (const char*)dev + pc.b,
-                                       pc.e - pc.b, cudaMemcpyDeviceToHost, c->copy_stream));
-            TS_CUDA(c, cudaEventRecord(c->stage_events[sl], c->copy_stream));
-            return TS_OK;
-        };
-        ts_status s;
-        for (size_t k = 0; k + 1 < (size_t)STAGE_SLOTS && k < pieces.size(); ++k)
-            if ((s = issue(k)) != TS_OK) return s;
-        for (size_t k = 0; k < pieces.size(); ++k) {
-            if (k + STAGE_SLOTS - 1 < pieces.size())
-                if ((s = issue(k + STAGE_SLOTS - 1)) != TS_OK) return s;
-            const int sl = (int)(k % STAGE_SLOTS);
-            TS_CUDA(c, cudaEventSynchronize(c->stage_events[sl]));
-            c->copy_pool->copy((char*)host + pieces[k].b, (const char*)c->stage + (size_t)sl * STAGE_SLOT_BYTES,
-                               pieces[k].e - pieces[k].b);
-        }
-        return TS_OK;
-    }
-};
-
 // The chunks, the merge tree over their sorted runs, and the copies of one
 // pipelined call. sort_chunk(i, b, e) enqueues chunk i's sort (into its
 // level-0 run); merge(L, r1, r2, last) enqueues the merge of two level-L
@@ -265,21 +137,6 @@ ts_status run_pipeline(ts_ctx* c, size_t n, CopyIn copy_chunk, SortChunk sort_ch
     }
     mark(c, "end");
     return TS_OK;
-}
-
-// the events a pipelined call records: [C] chunks in, [PIPE_SLICES] output
-// slices merged, then "stream reached the call" and "copies out done"
-inline cudaEvent_t* slice_events(ts_ctx* c) { return c->pipe_events.data() + c->transfer_chunks; }
-inline cudaEvent_t done_event(ts_ctx* c) { return c->pipe_events[c->transfer_chunks + PIPE_SLICES + 1]; }
-
-// whatever failed, nothing may still copy into or out of the caller's slices
-inline ts_status pipeline_end(ts_ctx* c, ts_status s) {
-    if (s != TS_OK) {
-        if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
-        cudaStreamSynchronize(c->stream);
-        return s;
-    }
-    return finish(c);
 }
 
 // Sort the host slice h[0, n) with the copies overlapped (c->transfer_chunks

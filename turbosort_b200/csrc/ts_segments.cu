@@ -9,6 +9,7 @@
 
 #include "ts_engine.cuh"
 #include "ts_segmented.cuh"
+#include "ts_transfer.h"
 
 namespace ts {
 namespace {
@@ -126,6 +127,82 @@ ts_status sort_segments_device(ts_ctx* c, U* d, size_t n, const unsigned long lo
     return TS_OK;
 }
 
+// Host segments with the copies overlapped. Segments are independent, so
+// the batch goes as transfer_chunks groups of whole segments (about equal
+// key counts): group g is sorted as soon as it is on the device, while later
+// groups still cross. With a pinned slice each sorted group goes back on a
+// stream of its own at once, so copies in and out run together (PCIe carries
+// both directions); a pageable slice goes through the staging slots, in
+// first and back afterwards, since this thread does those copies itself.
+template <typename U, int XF>
+ts_status pipeline_segments(ts_ctx* c, U* data, size_t n, const uint64_t* offsets, size_t n_seg,
+                            const std::vector<size_t>& huge) {
+    const int G = c->transfer_chunks;
+    ts_status s;
+    if ((s = grow(c, c->keys, n * sizeof(U) + 16, "keys")) != TS_OK) return s;
+    if ((s = seg_prepare<U, XF>(c, n, n_seg)) != TS_OK) return s;
+    if ((s = pipe_resources(c, (size_t)2 * G + PIPE_SLICES + 2)) != TS_OK) return s;
+    U* d = (U*)c->keys.p;
+    unsigned long long* d_off = (unsigned long long*)((char*)c->seg.p + SegLayout::make(n_seg).offs_off);
+    SegMethods m;
+    for (int b = 0; b < SEG_BLOCK_BINS; ++b) m.m[b] = c->seg_methods[width_index(sizeof(U))][b];
+    // group g: segments [sg[g], sg[g + 1]), keys [kg[g], kg[g + 1]) (all n keys are copied)
+    std::vector<size_t> sg(G + 1), kg(G + 1);
+    for (int g = 0; g <= G; ++g) {
+        const uint64_t want = offsets[0] + (offsets[n_seg] - offsets[0]) * (uint64_t)g / G;
+        sg[g] = g == G ? n_seg : (size_t)(std::lower_bound(offsets, offsets + n_seg, want) - offsets);
+        if (g > 0) sg[g] = std::max(sg[g], sg[g - 1]);
+        kg[g] = g == 0 ? 0 : g == G ? n : offsets[sg[g]];
+    }
+    cudaEvent_t* ev = c->pipe_events.data();                    // [G] group g is on the device
+    cudaEvent_t* sorted = ev + G + PIPE_SLICES + 2;             // [G] group g is sorted
+    Transfer tin(c, data), tout(c, data, c->out_stream);
+    TS_CUDA(c, cudaEventRecord(ev[G + PIPE_SLICES], c->stream));
+    TS_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ev[G + PIPE_SLICES], 0));
+    TS_CUDA(c, cudaStreamWaitEvent(c->out_stream, ev[G + PIPE_SLICES], 0));
+    mark(c, "pipeline");
+    if ((s = tin.in(d_off, offsets, (n_seg + 1) * 8)) != TS_OK) return s;
+    auto copy_in = [&](int g) -> ts_status {
+        if (g >= G) return TS_OK;
+        ts_status st = tin.in(d + kg[g], data + kg[g], (kg[g + 1] - kg[g]) * sizeof(U));
+        if (st != TS_OK) return st;
+        TS_CUDA(c, cudaEventRecord(ev[g], c->copy_stream));
+        return TS_OK;
+    };
+    if ((s = copy_in(0)) != TS_OK) return s;
+    if ((s = copy_in(1)) != TS_OK) return s;
+    size_t next_huge = 0;
+    size_t end[64];
+    for (int g = 0; g < G; ++g) {
+        TS_CUDA(c, cudaStreamWaitEvent(c->stream, ev[g], 0));
+        if (sg[g + 1] > sg[g] &&
+            (s = seg_enqueue<U, XF>(c, d, n, d_off + sg[g], sg[g + 1] - sg[g], kHostHugeSegment, m)) != TS_OK)
+            return s;
+        for (; next_huge < huge.size() && huge[next_huge] < sg[g + 1]; ++next_huge) {
+            const size_t i = huge[next_huge];
+            if ((s = sort_keys_device<U, XF>(c, d + offsets[i], offsets[i + 1] - offsets[i],
+                                             (U*)c->alt.p + offsets[i])) != TS_OK)
+                return s;
+        }
+        TS_CUDA(c, cudaEventRecord(sorted[g], c->stream));
+        end[g] = kg[g + 1] * sizeof(U);
+        if (!tout.pageable && kg[g + 1] > kg[g]) {
+            TS_CUDA(c, cudaStreamWaitEvent(c->out_stream, sorted[g], 0));
+            TS_CUDA(c, cudaMemcpyAsync(data + kg[g], d + kg[g], (kg[g + 1] - kg[g]) * sizeof(U), cudaMemcpyDeviceToHost,
+                                       c->out_stream));
+        }
+        if ((s = copy_in(g + 2)) != TS_OK) return s;
+    }
+    mark(c, "end");
+    if (tout.pageable) {
+        tout.st = c->copy_stream;  // behind every staged copy in
+        if ((s = tout.out(data, d, end, sorted, G)) != TS_OK) return s;
+    }
+    TS_CUDA(c, cudaEventRecord(done_event(c), tout.st));
+    TS_CUDA(c, cudaStreamWaitEvent(c->stream, done_event(c), 0));
+    return TS_OK;
+}
+
 template <typename T, typename U, int XF>
 ts_status host_segments(ts_ctx* c, T* data, size_t n, const uint64_t* offsets, size_t n_seg) {
     if (!c) return TS_ERR_INVALID;
@@ -137,6 +214,8 @@ ts_status host_segments(ts_ctx* c, T* data, size_t n, const uint64_t* offsets, s
             return fail(c, TS_ERR_INVALID, "segment offsets must be non-decreasing and end within the slice");
         if (offsets[i + 1] - offsets[i] > kHostHugeSegment) huge.push_back(i);
     }
+    if (c->transfer_chunks > 1 && n * sizeof(U) >= c->transfer_min_bytes && n_seg >= 2)
+        return pipeline_end(c, pipeline_segments<U, XF>(c, (U*)data, n, offsets, n_seg, huge));
     ts_status s;
     if ((s = grow(c, c->keys, n * sizeof(U) + 16, "keys")) != TS_OK) return s;
     if ((s = seg_prepare<U, XF>(c, n, n_seg)) != TS_OK) return s;
