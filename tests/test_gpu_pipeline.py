@@ -223,6 +223,21 @@ def test_segments_pipeline_matches_oracle(ts, t):
     ctx.close()
 
 
+def test_learned_sort_of_a_pageable_slice(ts):
+    """The learned sort needs every key before it partitions, so its host
+    copies do not overlap it; a pageable slice crosses through the staging
+    slots (here larger than the ring) and comes back sorted."""
+    from turbosort_b200 import workloads as W
+
+    ctx = ts.Context(0)
+    ctx.transfer_pipeline(8, 0)
+    for a in (W.lognormal_f64((1 << 24) + 3), W.gauss_mix_u64(1 << 21)):
+        got = a.copy()
+        ts.sort_learned(got, ctx=ctx)
+        assert got.tobytes() == O.sort(a).tobytes(), a.dtype
+    ctx.close()
+
+
 def test_rejects_bad_chunk_counts(ts):
     ctx = ts.Context(0)
     for bad in (0, 3, 12, 128):

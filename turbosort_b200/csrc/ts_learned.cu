@@ -8,6 +8,7 @@
 
 #include "ts_engine.cuh"
 #include "ts_learned.cuh"
+#include "ts_transfer.h"
 #include "ts_segmented.cuh"
 
 namespace ts {
@@ -240,6 +241,25 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     return done(s);
 }
 
+template <typename U, int XF>
+static ts_status staged_learned(ts_ctx* c, Transfer& t, U* data, U* d, size_t n, const ts_learned_params* P,
+                                ts_learned_stats* st) {
+    cudaEvent_t* ev = c->pipe_events.data();
+    ts_status s;
+    TS_CUDA(c, cudaEventRecord(ev[0], c->stream));
+    TS_CUDA(c, cudaStreamWaitEvent(t.st, ev[0], 0));
+    if ((s = t.in(d, data, n * sizeof(U))) != TS_OK) return s;
+    TS_CUDA(c, cudaEventRecord(ev[1], t.st));
+    TS_CUDA(c, cudaStreamWaitEvent(c->stream, ev[1], 0));
+    if ((s = learned_sort_device<U, XF>(c, d, n, P, st)) != TS_OK) return s;
+    TS_CUDA(c, cudaEventRecord(slice_events(c)[0], c->stream));
+    const size_t end = n * sizeof(U);
+    if ((s = t.out(data, d, &end, slice_events(c), 1)) != TS_OK) return s;
+    TS_CUDA(c, cudaEventRecord(done_event(c), t.st));
+    TS_CUDA(c, cudaStreamWaitEvent(c->stream, done_event(c), 0));
+    return TS_OK;
+}
+
 template <typename T, typename U, int XF>
 static ts_status host_learned(ts_ctx* c, T* data, size_t n, const ts_learned_params* P, ts_learned_stats* st) {
     if (!c) return TS_ERR_INVALID;
@@ -248,6 +268,13 @@ static ts_status host_learned(ts_ctx* c, T* data, size_t n, const ts_learned_par
     ts_status s;
     if ((s = grow(c, c->keys, n * sizeof(U) + 16, "keys")) != TS_OK) return s;
     U* d = (U*)c->keys.p;
+    if (c->transfer_chunks > 1 && n * sizeof(U) >= c->transfer_min_bytes) {
+        // the partition needs every key, so nothing overlaps the copies; a
+        // pageable slice still crosses through the staging slots
+        if ((s = pipe_resources(c, (size_t)c->transfer_chunks + PIPE_SLICES + 2)) != TS_OK) return s;
+        Transfer t(c, data);
+        if (t.pageable) return pipeline_end(c, staged_learned<U, XF>(c, t, (U*)data, d, n, P, st));
+    }
     TS_CUDA(c, cudaMemcpyAsync(d, data, n * sizeof(U), cudaMemcpyHostToDevice, c->stream));
     if ((s = learned_sort_device<U, XF>(c, d, n, P, st)) != TS_OK) return s;
     TS_CUDA(c, cudaMemcpyAsync(data, d, n * sizeof(U), cudaMemcpyDeviceToHost, c->stream));
