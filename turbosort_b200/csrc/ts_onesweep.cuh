@@ -192,6 +192,22 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
     // and for pairs that is a compile-time choice (TAGGED: the tile body is
     // built for both); a signed key's transform is one XOR, done with a mask
     // that is the sign bit only in the first or last pass.
+    // The digit of a key. With 8-bit digits it is one byte of the key: a
+    // byte permute (one instruction) with a selector fixed for the launch
+    // takes it out zero-extended, where a variable shift and a mask take two
+    // (and a 64-bit shift more); 64-bit keys first pick the 32-bit half.
+    const uint32_t byte_sel = 0x4440u | (uint32_t)((shift & 31) >> 3);
+    auto dig = [&](U k) -> uint32_t {
+        if constexpr (BITS == 8) {
+            uint32_t w;
+            if constexpr (sizeof(U) == 8) w = shift >= 32 ? (uint32_t)((uint64_t)k >> 32) : (uint32_t)k;
+            else w = (uint32_t)k;
+            return __byte_perm(w, 0u, byte_sel);
+        } else {
+            return digit_of(k, shift, MASK);
+        }
+    };
+
     constexpr bool TAGGED = XF == 2 || PAIRS;
     constexpr U SIGN = (U)((U)1 << (8 * sizeof(U) - 1));
     const U first_mask = (XF == 1 && first) ? SIGN : (U)0;
@@ -234,7 +250,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
             for (int i = 0; i < IPT; ++i) {
                 if (FULL || wbase + i * 32 < tile_n) {
                     const U k = load_key(kb[wbase + i * 32]);
-                    atomicAdd(&my_cnt[digit_of(k, shift, MASK)], 1u);
+                    atomicAdd(&my_cnt[dig(k)], 1u);
                 }
             }
         }
@@ -289,7 +305,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                 const int idx = wbase + i * 32;
                 const bool valid = FULL || idx < tile_n;
                 const U k = load_key(kb[FULL ? idx : min(idx, TILE - 1)]);
-                const uint32_t d = digit_of(k, shift, MASK);
+                const uint32_t d = dig(k);
                 uint32_t peers;
                 if ((i % MATCH_MOD) < MATCH_CNT) peers = __match_any_sync(0xffffffffu, d);
                 else peers = pm.peers(d);
@@ -369,7 +385,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                 const int s = i * THREADS + tid;
                 if ((TILE % THREADS == 0 || i < SCATTER_IT - 1 || s < TILE) && (FULL || s < tile_n)) {
                     const U k = sk[s];
-                    const OFF p = gbase[digit_of(k, shift, MASK)] + (OFF)s;
+                    const OFF p = gbase[dig(k)] + (OFF)s;
                     if (write_keys) {
                         if constexpr (LAST) dst[p] = from_key<U, XF>(k);
                         else if constexpr (XF == 1) dst[p] = (U)(k ^ last_mask);
