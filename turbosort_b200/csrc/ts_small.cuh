@@ -18,9 +18,11 @@ namespace ts {
 constexpr int SMALL_MAX = 4096;
 constexpr int SMALL_THREADS = 1024;
 
+// `in` and `out` may be the same array (the keys are all in shared memory
+// before the first write), so neither is declared restrict.
 template <typename U, int XF, bool PAIRS>
-__global__ void __launch_bounds__(SMALL_THREADS) k_small_sort(const U* __restrict__ in, U* __restrict__ out,
-                                                              uint32_t* __restrict__ order, int n, int write_keys) {
+__global__ void __launch_bounds__(SMALL_THREADS) k_small_sort(const U* in, U* out, uint32_t* __restrict__ order, int n,
+                                                              int write_keys) {
     __shared__ U sk[SMALL_MAX];
     __shared__ uint32_t sv[PAIRS ? SMALL_MAX : 1];
     int p2 = 1;
