@@ -108,11 +108,10 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
 
     mark(c, "scan");
     TS_CUDA(c, cudaMemsetAsync(meta, 0, m.zero_bytes(), c->stream));
-    TS_CUDA(c, cudaMemsetAsync(lb, 0, lb_words * 4, c->stream));
     {
         constexpr int T = 256;
         const int grid = c->sm_count * 4;
-        k_scan<U, XF, T><<<grid, T, 0, c->stream>>>(in, n, C::BITS, ND, st, vec_ok);
+        k_scan<U, XF, T><<<grid, T, 0, c->stream>>>(in, n, C::BITS, ND, st, vec_ok, (uint4*)lb, lb_words / 4);
         ++c->launches;
     }
     mark(c, "histogram");
@@ -210,9 +209,7 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
                 return st;
             mark(c, "finish");
             const int grid = c->sm_count * 4;
-            k_copy_back<U><<<grid, 512, 0, c->stream>>>(plan, d_alt, d_data, n, aligned16(d_alt) && aligned16(d_data));
-            ++c->launches;
-            k_reverse<U><<<grid, 512, 0, c->stream>>>(plan, d_data, n);
+            k_finish_keys<U><<<grid, 512, 0, c->stream>>>(plan, d_alt, d_data, n, aligned16(d_alt) && aligned16(d_data));
             ++c->launches;
             mark(c, "end");
             return TS_OK;

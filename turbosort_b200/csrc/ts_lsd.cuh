@@ -14,9 +14,9 @@
 //               transform (src/key.rs:135-197) is fused into the first load
 //               and the last store. Optionally carries a u32 position (the
 //               stable order() of src/by_key.rs:254-310).
-//   k_finish    copy-back for an odd pass count (src/radix/mod.rs:265-267),
-//               the reversal of descending input, iota for an order that
-//               needed no pass
+//   k_finish_keys  copy-back for an odd pass count (src/radix/mod.rs:265-267)
+//               or the reversal of descending input; k_iota_if_unsorted, the
+//               order of an input that needed no pass
 #pragma once
 
 #include <type_traits>
@@ -48,7 +48,12 @@ __device__ __forceinline__ bool all_digits_vary(unsigned long long diff, int bit
 // ---------------------------------------------------------------------------
 template <typename U, int XF, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_scan(const U* __restrict__ src, size_t n, int bits, int nd,
-                                                  ScanState* __restrict__ st, int vec_ok) {
+                                                  ScanState* __restrict__ st, int vec_ok, uint4* __restrict__ lb,
+                                                  size_t lb_vecs) {
+    // the first onesweep launch's look-back region starts at zero (each
+    // launch clears the next one's); done before any warp can leave
+    for (size_t i = (size_t)blockIdx.x * THREADS + threadIdx.x; i < lb_vecs; i += (size_t)gridDim.x * THREADS)
+        lb[i] = make_uint4(0u, 0u, 0u, 0u);
     using V = Vec16<U>;
     constexpr int VN = V::N;
     constexpr int UNROLL = 4;
@@ -242,12 +247,22 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
 // ---------------------------------------------------------------------------
 // Finishing kernels, each a no-op unless the plan calls for it.
 // ---------------------------------------------------------------------------
+// The end of a key sort, in one launch: the copy back for an odd count of
+// live passes (src/radix/mod.rs:265-267), or the reversal of descending
+// input (src/presorted.rs:15-65), as the plan says; nothing otherwise.
 template <typename U>
-__global__ void k_copy_back(const Plan* __restrict__ plan, const U* __restrict__ from, U* __restrict__ to, size_t n,
-                            int vec_ok) {
+__global__ void k_finish_keys(const Plan* __restrict__ plan, const U* from, U* to, size_t n, int vec_ok) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    if (plan->mode == MODE_REVERSE) {
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 2; i += stride) {
+            const U x = to[i];
+            to[i] = to[n - 1 - i];
+            to[n - 1 - i] = x;
+        }
+        return;
+    }
     if (plan->mode != MODE_SORT || (plan->n_live & 1) == 0) return;
     using V = Vec16<U>;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
     if (vec_ok) {
         const size_t nv = n / V::N;
         const uint4* f = reinterpret_cast<const uint4*>(from);
@@ -256,17 +271,6 @@ __global__ void k_copy_back(const Plan* __restrict__ plan, const U* __restrict__
         for (size_t i = nv * V::N + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) to[i] = from[i];
     } else {
         for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) to[i] = from[i];
-    }
-}
-
-template <typename U>
-__global__ void k_reverse(const Plan* __restrict__ plan, U* __restrict__ data, size_t n) {
-    if (plan->mode != MODE_REVERSE) return;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 2; i += stride) {
-        const U x = data[i];
-        data[i] = data[n - 1 - i];
-        data[n - 1 - i] = x;
     }
 }
 
