@@ -42,7 +42,7 @@ __device__ __forceinline__ bool all_digits_vary(unsigned long long diff, int bit
 }
 
 // ---------------------------------------------------------------------------
-// k_scan: OR of (key ^ first key) and the two sortedness flags. Warps leave
+// k_scan: OR of (key ^ first key) and the two sortedness flags. CTAs leave
 // as soon as every digit has varied and both directions are disproved,
 // which random input does in its first chunk.
 // ---------------------------------------------------------------------------
@@ -57,8 +57,11 @@ __global__ void __launch_bounds__(THREADS) k_scan(const U* __restrict__ src, siz
     using V = Vec16<U>;
     constexpr int VN = V::N;
     constexpr int UNROLL = 4;
+    __shared__ unsigned long long s_diff[THREADS / 32];
+    __shared__ unsigned s_flags[THREADS / 32];
+    __shared__ int s_stop;
     const U first = to_key<U, XF>(src[0]);
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long diff = 0, published = 0;
     unsigned flags = 0, pub_flags = 0;
     const size_t per_iter = (size_t)THREADS * VN * UNROLL;
@@ -98,27 +101,42 @@ __global__ void __launch_bounds__(THREADS) k_scan(const U* __restrict__ src, siz
                 }
             }
         }
-        // warp-level merge, publish what is new, and read the global state
+        // merge over the CTA (every warp runs the same iterations), then one
+        // thread reads the global state and publishes only what it lacks: once
+        // the input is known to be unsorted with every digit varying, CTAs
+        // leave without touching the two shared words (thousands of atomics
+        // on one address would serialise)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             diff |= __shfl_xor_sync(0xffffffffu, diff, o);
             flags |= __shfl_xor_sync(0xffffffffu, flags, o);
         }
-        int stop = 0;
         if (lane == 0) {
-            if (diff & ~published) {
-                atomicOr(&st->diff, diff);
-                published |= diff;
-            }
-            if (flags & ~pub_flags) {
-                atomicOr(&st->flags, flags);
-                pub_flags |= flags;
+            s_diff[warp] = diff;
+            s_flags[warp] = flags;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 0; w < THREADS / 32; ++w) {
+                diff |= s_diff[w];
+                flags |= s_flags[w];
             }
             unsigned long long g = ld_volatile_u64(&st->diff);
             unsigned gf = ld_volatile_u32(&st->flags);
-            stop = (gf == (SCAN_NOT_ASC | SCAN_NOT_DESC)) && all_digits_vary(g, bits, nd);
+            if (diff & ~(published | g)) {
+                atomicOr(&st->diff, diff);
+                g |= diff;
+            }
+            if (flags & ~(pub_flags | gf)) {
+                atomicOr(&st->flags, flags);
+                gf |= flags;
+            }
+            published |= diff;
+            pub_flags |= flags;
+            s_stop = (gf == (SCAN_NOT_ASC | SCAN_NOT_DESC)) && all_digits_vary(g, bits, nd);
         }
-        if (__shfl_sync(0xffffffffu, stop, 0)) return;
+        __syncthreads();
+        if (s_stop) return;
     }
 }
 
