@@ -53,6 +53,10 @@ def test_status_strings_and_no_device_path():
     assert L.ts_status_str(2) == b"length mismatch"
     # null context is rejected without touching a device
     assert L.ts_sort_u32(None, None, 0) == 6
+    assert L.ts_ctx_transfer_pipeline(None, 8, 0) == 6
+    assert L.ts_sort_keys_order_u64(None, None, 0, None) == 6
+    assert L.ts_apply_order(None, None, 0, 16, None, 0) == 6
+    assert L.ts_sort_segments_u32(None, None, 0, None, 0) == 6
 
 
 def test_learned_structs_match_the_header():
