@@ -1,6 +1,7 @@
-// ts_transfer.h — the copies of a pipelined host-slice call: a second
-// stream, events, and for pageable host memory the context's pinned staging
-// slots with the copy pool's threads (ts_staging.h).
+// ts_transfer.h — the copies of a pipelined host-slice call: two copy
+// streams beside the context's stream (copies in, and copies out that must
+// run while copies in continue), events, and for pageable host memory the
+// context's pinned staging slots with the copy pool's threads (ts_staging.h).
 //
 // A pageable host slice cannot be a DMA source or target; the driver would
 // copy it through its own pinned buffer on the calling thread at about a
