@@ -1,7 +1,7 @@
 // ts_staging.h — host threads that copy between a caller's pageable memory
 // and the context's pinned staging slots.
 //
-// A copy from pageable host memory cannot be a DMA of its own: the driver
+// A copy from pageable host memory cannot be a DMA of its own: the CUDA driver
 // copies it through its own pinned buffer on the calling thread, at about a
 // quarter of what PCIe carries. The host-slice pipeline instead copies each
 // piece into one of its pinned slots with several threads at once, and the

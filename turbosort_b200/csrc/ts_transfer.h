@@ -3,7 +3,7 @@
 // run while copies in continue), events, and for pageable host memory the
 // context's pinned staging slots with the copy pool's threads (ts_staging.h).
 //
-// A pageable host slice cannot be a DMA source or target; the driver would
+// A pageable host slice cannot be a DMA source or target; the CUDA driver would
 // copy it through its own pinned buffer on the calling thread at about a
 // quarter of the PCIe rate. Such a slice goes through STAGE_SLOTS pinned
 // slots instead: the copy threads fill a slot while the DMA of the previous
@@ -26,7 +26,7 @@ constexpr int STAGE_SLOTS = 4;                     // pinned staging slots for p
 constexpr size_t STAGE_SLOT_BYTES = (size_t)32 << 20;
 
 // the pinned slots, their events and the copy threads; false if pinned
-// memory cannot be had (the slice then takes the driver's own staging)
+// memory cannot be had (the slice then takes the CUDA driver's own staging)
 inline bool stage_resources(ts_ctx* c) {
     if (!c->stage) {
         if (cudaHostAlloc(&c->stage, STAGE_SLOTS * STAGE_SLOT_BYTES, cudaHostAllocDefault) != cudaSuccess) {
