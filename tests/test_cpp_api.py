@@ -48,3 +48,21 @@ def test_copy_pool_copies_every_byte(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.strip() == "ok"
+
+
+def test_copy_pool_has_no_data_race(tmp_path):
+    """The same program under ThreadSanitizer: the pool's hand-off between the
+    caller and its workers (one mutex, two condition variables) is race-free."""
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no g++")
+    exe = str(tmp_path / "copy_pool_tsan")
+    r = subprocess.run([cxx, "-std=c++17", "-O1", "-g", "-fsanitize=thread", "-pthread", "-I",
+                        os.path.join(ROOT, "turbosort_b200", "csrc"),
+                        os.path.join(ROOT, "tests", "cpp", "copy_pool_test.cpp"), "-o", exe],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.skip("no ThreadSanitizer runtime: " + r.stderr[-200:])
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert "ThreadSanitizer" not in r.stderr, r.stderr[-2000:]
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr[-2000:]
