@@ -10,6 +10,8 @@ against the oracle.
   correlated top bytes, 1000 distinct values, heavy tail, pipe organ, equal
   buckets) at tier and tile boundaries, for every key width.
 """
+import zlib
+
 import numpy as np
 import pytest
 
@@ -94,10 +96,53 @@ SHAPES = ["split_top_bit", "correlated_top", "distinct_1000", "heavy_tail", "pip
 
 @pytest.mark.parametrize("t", ["u16", "u32", "i32", "f32", "u64", "i64", "f64"])
 def test_structured_shapes(ts, t):
-    rng = np.random.default_rng(abs(hash(("shapes", t))) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(b"shapes " + t.encode()))
     for n in (4095, 4097, 11264, 11265, 65537, 300_001):
         for shape in SHAPES:
             a = structured(t, n, shape, rng)
+            got = a.copy()
+            ts.sort(got)
+            assert got.tobytes() == O.sort(a).tobytes(), (t, n, shape)
+            order = ts.keys_order(a)
+            assert order.tobytes() == O.sort_by_key_order(a).tobytes(), (t, n, shape, "order")
+
+
+def adversarial(t, n, shape, rng):
+    """Patterns aimed at radix sorts (the crate's adversarial cases,
+    tests/correctness.rs:575-635): digit-aligned sawtooth, alternating
+    extremes, one outlier, keys differing in one byte only."""
+    kd = O.KEY_DTYPE[t]
+    w = np.dtype(kd).itemsize * 8
+    i = np.arange(n, dtype=np.uint64)
+    full = np.uint64((1 << w) - 1 if w < 64 else 2**64 - 1)
+    if shape == "sawtooth_256":
+        b = i % np.uint64(256)
+    elif shape == "sawtooth_65536":
+        b = i % np.uint64(65536)
+    elif shape == "alternating_extremes":
+        b = np.where(i % np.uint64(2) == 0, np.uint64(0), full)
+    elif shape == "one_outlier":
+        b = np.full(n, 7, dtype=np.uint64)
+        b[n // 2] = full
+    elif shape == "top_byte_only":
+        b = rng.integers(0, 256, size=n, dtype=np.uint64) << np.uint64(w - 8)
+    elif shape == "bottom_byte_only":
+        b = rng.integers(0, 256, size=n, dtype=np.uint64) | (full & ~np.uint64(0xFF))
+    else:
+        raise ValueError(shape)
+    return (b & full).astype(kd).view(O.NP_DTYPE[t])
+
+
+ADVERSARIAL = ["sawtooth_256", "sawtooth_65536", "alternating_extremes", "one_outlier", "top_byte_only",
+               "bottom_byte_only"]
+
+
+@pytest.mark.parametrize("t", ["u16", "u32", "i32", "f32", "u64", "f64"])
+def test_adversarial_shapes(ts, t):
+    rng = np.random.default_rng(zlib.crc32(b"adv " + t.encode()))
+    for n in (4096, 4097, 65536, 300_000):
+        for shape in ADVERSARIAL:
+            a = adversarial(t, n, shape, rng)
             got = a.copy()
             ts.sort(got)
             assert got.tobytes() == O.sort(a).tobytes(), (t, n, shape)
