@@ -5,6 +5,7 @@ and docs by tests/golden/make_golden.py (file:line there). The oracle is also
 checked against numpy sorts of the radix keys, an independent implementation.
 """
 import itertools
+import os
 
 import numpy as np
 import pytest
@@ -169,3 +170,26 @@ def test_oracle_matches_numpy(t):
 def test_sort_with_buffer_too_small():
     _, st = O.sort_with_buffer(np.arange(10, dtype=np.uint32), buf_len=9)
     assert st == 1
+
+
+def test_oracle_under_address_and_undefined_behaviour_sanitizers(tmp_path):
+    """The C oracle built with ASan and UBSan (leaks included) and driven
+    through every key type, the crate's tier-boundary sizes and shapes, by a
+    driver that checks each result itself."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("no gcc")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "oracle_sanitize")
+    r = subprocess.run([cc, "-std=c11", "-O1", "-g", "-fsanitize=address,undefined", "-fno-sanitize-recover=undefined",
+                        os.path.join(root, "oracle", "turbosort_oracle.c"),
+                        os.path.join(root, "tests", "cpp", "oracle_sanitize.c"), "-lpthread", "-lm", "-o", exe],
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.skip("no sanitizer runtime: " + r.stderr[-200:])
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300,
+                       env={**os.environ, "ASAN_OPTIONS": "detect_leaks=1"})
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr[-3000:]
