@@ -282,3 +282,20 @@ def test_repeated_sorts_of_one_buffer(ts, t):
     assert len(set(launches)) == 1, launches  # a replay counts the launches it holds
     ctx.close()
     torch.cuda.synchronize()
+
+
+def test_out_of_memory_is_reported_and_the_context_stays_usable(ts):
+    """Forced allocation failure: scratch for 2^40 u64 keys (8 TiB) cannot be
+    had; the call reports TS_ERR_OOM with the size it wanted (no fault, no
+    sticky error), and the same context sorts as before afterwards."""
+    ctx = ts.Context(0)
+    a = np.arange(100_000, dtype=np.uint32)[::-1].copy()
+    ts.sort(a, ctx)
+    with pytest.raises(ts.TurbosortError) as e:
+        ctx.reserve(1 << 40, 8)
+    assert e.value.status == 5 and "cannot reserve" in str(e.value)
+    b = np.random.default_rng(1).integers(0, 2**32, size=300_000, dtype=np.uint64).astype(np.uint32)
+    got = b.copy()
+    ts.sort(got, ctx)
+    assert got.tobytes() == O.sort(b).tobytes()
+    ctx.close()
