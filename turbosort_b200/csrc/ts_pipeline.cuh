@@ -19,7 +19,10 @@
 // copy of chunk i + 2 is issued after the sort of chunk i and every copy out
 // after the last merge.
 //
-// Pageable host slices cross through pinned staging slots (ts_transfer.h).
+// The same chunks and merge tree (run_pipeline) serve sort_by_key's order()
+// (pipeline_order): a chunk's run is its stable order, and runs of positions
+// are merged by the keys they point to. Pageable host slices cross through
+// pinned staging slots (ts_transfer.h).
 #pragma once
 
 #include <algorithm>
@@ -139,8 +142,9 @@ ts_status run_pipeline(ts_ctx* c, size_t n, CopyIn copy_chunk, SortChunk sort_ch
     return TS_OK;
 }
 
-// Sort the host slice h[0, n) with the copies overlapped (c->transfer_chunks
-// a power of two, at least 2). Returns once the sorted keys are back in h.
+// Enqueue the sort of the host slice h[0, n) with the copies overlapped
+// (c->transfer_chunks a power of two, at least 2); the context's stream ends
+// behind the last copy out.
 template <typename U, int XF>
 ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
     ts_status s;
@@ -172,6 +176,7 @@ ts_status pipeline_body(ts_ctx* c, U* h, size_t n) {
     return TS_OK;
 }
 
+// The pipelined host sort: returns once the sorted keys are back in h.
 template <typename U, int XF>
 ts_status pipeline_sort(ts_ctx* c, U* h, size_t n) {
     return pipeline_end(c, pipeline_body<U, XF>(c, h, n));
@@ -181,7 +186,8 @@ ts_status pipeline_sort(ts_ctx* c, U* h, size_t n) {
 // src/by_key.rs:175-233) with the copies overlapped: each chunk's keys are
 // ordered by the device's stable LSD (positions within the chunk), and the
 // position runs are merged by the keys they point to, which stay where they
-// arrived. Returns once order[0, n) is back on the host.
+// arrived. Enqueues it all; the context's stream ends behind the last copy
+// of order[0, n) to the host.
 template <typename U, int XF>
 ts_status pipeline_order_body(ts_ctx* c, const U* h_keys, size_t n, uint32_t* h_order) {
     ts_status s;
@@ -223,6 +229,7 @@ ts_status pipeline_order_body(ts_ctx* c, const U* h_keys, size_t n, uint32_t* h_
     return TS_OK;
 }
 
+// The pipelined host order(): returns once order[0, n) is on the host.
 template <typename U, int XF>
 ts_status pipeline_order(ts_ctx* c, const U* h_keys, size_t n, uint32_t* h_order) {
     return pipeline_end(c, pipeline_order_body<U, XF>(c, h_keys, n, h_order));
