@@ -234,9 +234,11 @@ ts_status ts_lm_gradients(ts_ctx *ctx, const float *d_t, const float *d_y, size_
  * that. The sort runs on `stream` (a cudaStream_t, or NULL for the legacy
  * default stream) and the call returns when it is done. The first call on a
  * device looks up the array's address there; make that first call before any
- * stream capture. Calls share the array: calls that overlap on the GPU race,
- * so one process runs one at a time and callers in several processes or on
- * several streams must serialise them. */
+ * stream capture. Each process has one such array per device, shared by all
+ * of that process's calls on the device; they would race if they overlapped on
+ * the GPU, so the library runs them one at a time (each call blocks until its
+ * sort is done, also when it returns an error). Not for use across
+ * cudaDeviceReset, which discards the library's device code and the array. */
 #define TS_NOALLOC_MAX_KEYS ((size_t)1 << 22)
 ts_status ts_sort_dev_noalloc_u32(uint32_t *d_data, size_t n, void *stream);
 

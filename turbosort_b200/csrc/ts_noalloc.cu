@@ -11,11 +11,16 @@
 // lives in one file-scope device array of fixed size, loaded with the
 // library and held by every GPU that loads it until the process exits.
 //
-// The array is shared by all calls and keeps the last call's contents; the
-// sort clears what must start at zero (histograms, counters, the look-back
-// region, the error word) on the caller's stream before using it. Calls that
-// overlap on the GPU (from several host threads, or on several streams of one
-// device) race on the array and must be serialised by the caller.
+// Each process has its own copy of the array on each device, shared by every
+// call that process makes on that device; it keeps the last call's contents,
+// and the sort clears what must start at zero (histograms, counters, the
+// look-back region, the error word) on the caller's stream before using it.
+// Calls would race on the array if they overlapped on the GPU, so calls in
+// one process are serialised here (a lock held until the call's work has
+// finished on the GPU, on success and on every error return alike).
+// The array's device address is looked up once per device; after
+// cudaDeviceReset the library's device code and the array are gone, so the
+// entry point must not be used across a reset.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -94,17 +99,24 @@ extern "C" ts_status ts_sort_dev_noalloc_u32(uint32_t* d_data, size_t n, void* s
     if (s != TS_OK) return s;
     std::lock_guard<std::mutex> lock(g_mu);  // one call at a time per process
     c->stream = (cudaStream_t)stream;
+    // on an error after the first enqueue, wait for what was queued before
+    // the lock is released: the next call must not meet it on the array
+    auto drain = [&](ts_status st) {
+        cudaStreamSynchronize(c->stream);
+        cudaGetLastError();
+        return st;
+    };
     if (cudaMemsetAsync(c->d_error, 0, 4, c->stream) != cudaSuccess) {
         cudaGetLastError();
-        return TS_ERR_CUDA;
+        return drain(TS_ERR_CUDA);
     }
     s = ts::sort_keys_device<uint32_t, 0>(c, d_data, n, nullptr);
-    if (s != TS_OK) return s;
+    if (s != TS_OK) return drain(s);
     uint32_t err = 0;
     if (cudaMemcpyAsync(&err, c->d_error, 4, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess) {
         cudaGetLastError();
-        return TS_ERR_CUDA;
+        return drain(TS_ERR_CUDA);
     }
     if (err & ts::ERR_TIMEOUT) return TS_ERR_TIMEOUT;
     if (err & ts::ERR_BOUNDS) return TS_ERR_INTERNAL;
