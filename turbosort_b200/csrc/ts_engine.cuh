@@ -26,6 +26,9 @@ template <typename U, bool PAIRS>
 struct LsdCfg {
     static constexpr int BITS = 8;
     static constexpr int THREADS = 512;
+    // the first live pass of a keys-only sort ranks with shared atomics
+    // (k_onesweep, UNSTABLE1)
+    static constexpr bool UNSTABLE1 = true;
     // the largest tile for which two CTAs (one tile of keys and positions, the
     // staging tile, 32-bit per-warp counters) share one SM's shared memory:
     // the per-tile costs (look-back, counter scans) shrink per key as tiles
@@ -81,10 +84,9 @@ static inline bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
 // The LSD passes over `in` (n keys), writing through pp[0]/pp[1]; with PAIRS
 // the positions ping-pong through vpp and the last pass writes `vout`.
-template <typename U, int XF, bool PAIRS>
+template <typename U, int XF, bool PAIRS, typename C = LsdCfg<U, PAIRS>>
 static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0, uint32_t* vpp1, uint32_t* vout,
                          size_t n, int write_keys_last, Plan** plan_out) {
-    using C = LsdCfg<U, PAIRS>;
     constexpr int RADIX = C::RADIX, ND = C::ND, TILE = C::TILE;
     const size_t tiles = (n + TILE - 1) / TILE;
     const size_t max_portion_tiles = (size_t)(LB_VALUE / TILE);
@@ -129,8 +131,10 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     {
         using Sm = typename C::Smem;
         auto kern = n <= (size_t)0x7fffffff
-                        ? k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD, C::MATCH_CNT>
-                        : k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD, C::MATCH_CNT>;
+                        ? k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD,
+                                     C::MATCH_CNT, C::UNSTABLE1>
+                        : k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD,
+                                     C::MATCH_CNT, C::UNSTABLE1>;
         const int occ = occupancy(c, kern, C::THREADS, Sm::bytes);
         SweepArgs<U, PAIRS> a{};
         a.in = in;

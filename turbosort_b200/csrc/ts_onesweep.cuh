@@ -108,8 +108,15 @@ struct PeerMasks {
 // Items i with i % MATCH_MOD < MATCH_CNT find their equal digits with the
 // match.any instruction, which runs on a different pipe from the ballots; the
 // rest use PeerMasks. The split keeps both pipes busy.
+//
+// UNSTABLE1: the first live pass of a keys-only sort ranks with one shared
+// atomic per key instead of finding its equals. That pass has no input
+// order to keep: after it the keys need only be ordered by its digit, and
+// the later (stable) passes order keys of equal higher digits by it. Keys
+// equal in every bit are the same bit pattern, so their order is not
+// observable. With positions (PAIRS) every pass stays stable.
 template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
-          int MATCH_CNT>
+          int MATCH_CNT, bool UNSTABLE1 = false>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<U, PAIRS> a) {
     using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
     using OFF = typename std::conditional<BIG, long long, int>::type;
@@ -216,9 +223,10 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
     // One tile. FULL (a compile-time tag) drops every per-key bounds test:
     // only the last tile of a portion can be partial. FIRST is the
     // compile-time first-pass tag (false unless TAGGED).
-    auto process = [&](int t, int b, auto full_tag, auto first_tag) {
+    auto process = [&](int t, int b, auto full_tag, auto first_tag, auto unstable_tag) {
         constexpr bool FULL = decltype(full_tag)::value;
         constexpr bool FIRST = decltype(first_tag)::value;
+        constexpr bool UNST = decltype(unstable_tag)::value;
         auto load_key = [&](U k) -> U {
             if constexpr (FIRST) return to_key<U, XF>(k);
             else if constexpr (XF == 1 && !TAGGED) return (U)(k ^ first_mask);
@@ -298,7 +306,17 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
         }
         __syncthreads();
 
-        {
+        if constexpr (UNST) {
+            // ---- 3'. first pass of a keys-only sort: any order inside a digit
+#pragma unroll
+            for (int i = 0; i < IPT; ++i) {
+                const int idx = wbase + i * 32;
+                if (FULL || idx < tile_n) {
+                    const U k = load_key(kb[idx]);
+                    sk[atomicAdd(&my_cnt[dig(k)], 1u)] = k;
+                }
+            }
+        } else {
             // ---- 3. rank among equal digits in the warp and stage in sorted order
 #pragma unroll
             for (int i = 0; i < IPT; ++i) {
@@ -406,15 +424,22 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
     };
     auto run_tile = [&](int t, int b) {
         const bool full = a.portion_begin + (size_t)(t + 1) * TILE <= portion_end;
-        auto go = [&](auto first_tag) {
-            if (full) process(t, b, std::true_type{}, first_tag);
-            else process(t, b, std::false_type{}, first_tag);
+        auto go = [&](auto first_tag, auto unstable_tag) {
+            if (full) process(t, b, std::true_type{}, first_tag, unstable_tag);
+            else process(t, b, std::false_type{}, first_tag, unstable_tag);
         };
         if constexpr (TAGGED) {
-            if (first) go(std::true_type{});
-            else go(std::false_type{});
+            if (first) {
+                if constexpr (UNSTABLE1 && !PAIRS) go(std::true_type{}, std::true_type{});
+                else go(std::true_type{}, std::false_type{});
+            } else {
+                go(std::false_type{}, std::false_type{});
+            }
+        } else if constexpr (UNSTABLE1 && !PAIRS) {
+            if (first) go(std::false_type{}, std::true_type{});
+            else go(std::false_type{}, std::false_type{});
         } else {
-            go(std::false_type{});
+            go(std::false_type{}, std::false_type{});
         }
     };
 
