@@ -299,11 +299,22 @@ def bench_device(ts, torch, ctx, kind, dist, lg, steps, warmup, seed, dist_mod, 
     tm = ctx.timings()
     ctx.enable_timing(False)
     ctx.synchronize()
+    info = ctx.last_sort_info()
+    if info["tier"] == 3 and info["mode"] == 0:
+        live = info["passes"]  # the scatter passes that ran (diverting may leave out low digits)
     out = copies[-1].cpu().numpy().view(NP[kind])
     del copies
     ok = check_exact(out, expected_radix(host))
     torch.cuda.empty_cache()
-    return {"ms_total": ms, "launches": launches, "timings": tm, "ok": ok, "live": live, "n": n, "w": w}
+    return {"ms_total": ms, "launches": launches, "timings": tm, "ok": ok, "live": live, "n": n, "w": w,
+            "divert_shift": info.get("divert_shift", 0)}
+
+
+def sort_bytes_of(r: dict) -> int:
+    """Algorithmic bytes of one sort: one upfront read, a read and a write per
+    scatter pass, and one read of the keys to find the runs when it diverted."""
+    nw = r["n"] * r["w"]
+    return nw * (2 * r["live"] + 1) + (nw if r.get("divert_shift") else 0)
 
 
 def bench_small(ts, torch, ctx, kind, dist, lg, steps, warmup, seed):
@@ -603,7 +614,7 @@ def main() -> None:
     per_launch_ms = sweep_ms / live_launches if sweep_ms else None
     pass_bytes = n * w * 2
     achieved = pass_bytes / (per_launch_ms / 1e3) / 1e9 if per_launch_ms else None
-    sort_bytes = n * w * (2 * live + 1)
+    sort_bytes = sort_bytes_of(r)
     traffic = ncu_traffic(f"onesweep_{kind}_2p{lg}.md")
 
     line = {
@@ -619,7 +630,7 @@ def main() -> None:
             "frac": round(achieved / peak, 4) if achieved else None, "peak_source": peak_kind,
             "traffic": traffic, "algorithmic_bytes_per_launch": pass_bytes,
             "avg_launch_ms": round(per_launch_ms, 4) if per_launch_ms else None,
-            "live_passes": live,
+            "live_passes": live, "divert_shift": r["divert_shift"],
             "sort_bytes": sort_bytes,
             "sort_achieved_gbs": round(sort_bytes / (ms_step / 1e3) / 1e9, 1),
             "sort_frac": round(sort_bytes / (ms_step / 1e3) / 1e9 / peak, 4),
@@ -687,9 +698,10 @@ def main() -> None:
             rr = bench_device(ts, torch, ctx, k2, d2, l2, max(3, args.steps // 2), 3, 0x1234 + rank, None, rank,
                               world)
             st = rr["ms_total"] / max(3, args.steps // 2)
-            sb = rr["n"] * rr["w"] * (2 * rr["live"] + 1)
+            sb = sort_bytes_of(rr)
             ow = rr["timings"].get("onesweep", (0.0, 0))[0] / max(1, rr["live"] * max(3, args.steps // 2))
             bd[name] = {"gkeys_s": round(rr["n"] / (st / 1e3) / 1e9, 2), "ms": round(st, 4), "live_passes": rr["live"],
+                        "divert_shift": rr["divert_shift"],
                         "sort_frac": round(sb / (st / 1e3) / 1e9 / peak, 3),
                         "pass_frac": round(rr["n"] * rr["w"] * 2 / (ow / 1e3) / 1e9 / peak, 3) if ow else None,
                         "ok": rr["ok"]}

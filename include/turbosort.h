@@ -85,6 +85,27 @@ void ts_ctx_reset_timings(ts_ctx *ctx);
 /* Kernels this context has launched so far (all entry points). */
 unsigned long long ts_ctx_launches(const ts_ctx *ctx);
 
+/* What the context's last plain sort did (device or host entry point, or a
+ * chunk of a host-slice sort); waits for the context's stream. tier: 0 none
+ * yet, 1 the small-slice network (n <= 4096), 2 the one-byte counting sort,
+ * 3 the LSD passes. For tier 3: mode 0 sorted by passes, 1 input already
+ * ascending, 2 descending input reversed; passes and pass_digit[] (8-bit
+ * digit indices, least significant first) are the scatter passes that ran;
+ * divert_shift > 0 means the sort diverted (src/radix/divert.rs:38-81): only
+ * the digits from that bit up were sorted by passes, and the runs of keys
+ * sharing them were finished directly. */
+typedef struct ts_sort_info {
+    int32_t tier, mode, passes, divert_shift;
+    int32_t pass_digit[16];
+} ts_sort_info;
+ts_status ts_ctx_last_sort_info(ts_ctx *ctx, ts_sort_info *info);
+
+/* The diverting rule of the crate (src/radix/divert.rs:38-54) as the device
+ * applies it: how many of the lowest of n_live live digits need no pass, for
+ * len keys whose i-th live digit (least significant first) has its largest
+ * bucket max_bucket[i]. Host-side, for checks. */
+int ts_divert_skippable_digits(int n_live, uint64_t len, const uint64_t *max_bucket);
+
 #define TS_DECLARE_SORTS(SUF, T)                                                                     \
     /* turbosort::sort (src/lib.rs:99): ascending, in place. */                                       \
     ts_status ts_sort_##SUF(ts_ctx *ctx, T *data, size_t n);                                          \

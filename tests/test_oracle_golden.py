@@ -193,3 +193,22 @@ def test_oracle_under_address_and_undefined_behaviour_sanitizers(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300,
                        env={**os.environ, "ASAN_OPTIONS": "detect_leaks=1"})
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr[-3000:]
+
+
+def test_library_divert_rule_matches_the_crate(kat):
+    """The diverting rule the device plan applies (k_plan), called on the host
+    through the C ABI: the crate's own expected digit counts
+    (src/radix/divert.rs:124-148), then the oracle's restatement on random
+    histogram maxima."""
+    import turbosort_b200 as ts
+
+    for c in kat["skippable_digits"]:
+        got = ts.divert_skippable_digits(c["n_live"], c["len"], [c["max"]] * max(c["n_live"], 1))
+        assert got == c["expect"], c
+    rng = np.random.default_rng(77)
+    for _ in range(3000):
+        n_live = int(rng.integers(0, 9))
+        length = int(rng.integers(1, 1 << 40))
+        maxb = [int(rng.integers(1, length + 1)) if rng.random() < 0.3 else max(1, length >> int(rng.integers(0, 12)))
+                for _ in range(max(n_live, 1))]
+        assert ts.divert_skippable_digits(n_live, length, maxb) == O.skippable_digits(n_live, length, maxb)

@@ -29,6 +29,7 @@ __all__ = [
     "Context", "SortByKeyBuffer", "TurbosortError", "apply_order", "default_context", "lib", "sort",
     "sort_by_key", "sort_by_key_with_buffer", "sort_parallel", "sort_segments", "sort_with_buffer", "segments_autotune",
     "segments_methods", "TYPES", "LearnedParams", "LearnedStats", "learned_params", "lm_gradients", "sort_learned",
+    "SortInfo", "divert_skippable_digits",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -74,6 +75,22 @@ class LearnedStats(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SortInfo(ctypes.Structure):
+    """ts_sort_info: what the context's last plain sort did."""
+    _fields_ = [("tier", ctypes.c_int32), ("mode", ctypes.c_int32), ("passes", ctypes.c_int32),
+                ("divert_shift", ctypes.c_int32), ("pass_digit", ctypes.c_int32 * 16)]
+
+    def as_dict(self) -> dict:
+        return {"tier": self.tier, "mode": self.mode, "passes": self.passes, "divert_shift": self.divert_shift,
+                "pass_digit": list(self.pass_digit[:self.passes])}
+
+
+def divert_skippable_digits(n_live: int, length: int, max_buckets) -> int:
+    """The library's diverting rule (src/radix/divert.rs:38-54), host-side."""
+    arr = (ctypes.c_uint64 * max(1, len(max_buckets)))(*[int(x) for x in max_buckets])
+    return int(lib().ts_divert_skippable_digits(n_live, length, arr))
 
 
 class TurbosortError(RuntimeError):
@@ -148,6 +165,10 @@ def lib() -> ctypes.CDLL:
             L.ts_ctx_use_graphs.restype = st
             L.ts_ctx_launches.argtypes = [vp]
             L.ts_ctx_launches.restype = ctypes.c_ulonglong
+            L.ts_ctx_last_sort_info.argtypes = [vp, ctypes.POINTER(SortInfo)]
+            L.ts_ctx_last_sort_info.restype = st
+            L.ts_divert_skippable_digits.argtypes = [i, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+            L.ts_divert_skippable_digits.restype = i
             L.ts_apply_order.argtypes = [vp, vp, sz, sz, vp, sz]
             L.ts_apply_order.restype = st
             L.ts_apply_order_dev.argtypes = [vp, vp, sz, sz, vp, sz]
@@ -214,6 +235,12 @@ class Context:
         """Host-slice sorts of at least min_bytes cross PCIe as `chunks` pieces,
         sorted and merged on the device while the copies run (1 turns it off)."""
         self._check(lib().ts_ctx_transfer_pipeline(self._h, chunks, min_bytes))
+
+    def last_sort_info(self) -> dict:
+        """Tier, mode, scatter passes and divert shift of the last plain sort."""
+        info = SortInfo()
+        self._check(lib().ts_ctx_last_sort_info(self._h, ctypes.byref(info)))
+        return info.as_dict()
 
     def enable_timing(self, on: bool = True) -> None:
         self._check(lib().ts_ctx_enable_timing(self._h, int(on)))

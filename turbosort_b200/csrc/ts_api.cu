@@ -9,6 +9,7 @@
 #include <unordered_map>
 
 #include "ts_ctx.h"
+#include "ts_engine.cuh"
 #include "ts_gather.cuh"
 #include "ts_transfer.h"
 
@@ -284,7 +285,8 @@ void ts_ctx_destroy(ts_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     if (c->out_stream) cudaStreamSynchronize(c->out_stream);
-    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->gather, &c->seg,
+    for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->runs, &c->gather,
+                      &c->seg,
                       &c->learn, &c->pipe, &c->pipe_pos[0], &c->pipe_pos[1]})
         if (b->p) cudaFree(b->p);
     for (auto ev : c->pipe_events) cudaEventDestroy(ev);
@@ -405,6 +407,27 @@ void ts_ctx_reset_timings(ts_ctx* c) {
 }
 
 unsigned long long ts_ctx_launches(const ts_ctx* c) { return c ? c->launches : 0ull; }
+
+ts_status ts_ctx_last_sort_info(ts_ctx* c, ts_sort_info* info) {
+    if (!c || !info) return TS_ERR_INVALID;
+    std::memset(info, 0, sizeof *info);
+    info->tier = c->last_tier;
+    if (c->last_tier != 3 || !c->meta.p) return TS_OK;
+    Plan p{};
+    const MetaLayout m = MetaLayout::make(1, 1, 0);  // the plan's place does not depend on the sort
+    TS_CUDA(c, cudaMemcpyAsync(&p, (const char*)c->meta.p + m.plan_off, sizeof p, cudaMemcpyDeviceToHost, c->stream));
+    TS_CUDA(c, cudaStreamSynchronize(c->stream));
+    info->mode = p.mode;
+    info->passes = p.n_live;
+    info->divert_shift = p.divert_shift;
+    for (int i = 0; i < p.n_live && i < 16; ++i) info->pass_digit[i] = p.pass[i];
+    return TS_OK;
+}
+
+int ts_divert_skippable_digits(int n_live, uint64_t len, const uint64_t* max_bucket) {
+    if (n_live <= 0 || len == 0 || !max_bucket) return 0;
+    return skippable_digits(n_live, (unsigned long long)len, (const unsigned long long*)max_bucket);
+}
 
 #define TS_DEFINE_SORTS(SUF, T, U, XF)                                                              \
     ts_status ts_sort_##SUF(ts_ctx* c, T* data, size_t n) { return host_sort<T, U, XF>(c, data, n); } \

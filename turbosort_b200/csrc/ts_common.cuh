@@ -81,7 +81,8 @@ struct Plan {
     int mode;
     int n_live;                  // live digit passes, least significant first
     int pass[MAX_PASSES];        // digit index of the j-th live pass
-    int pad[2];
+    int divert_shift;            // > 0: only digits from this bit up were sorted; runs left to finish
+    int pad;
 };
 
 // ---------------------------------------------------------------------------

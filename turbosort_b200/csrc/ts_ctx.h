@@ -35,6 +35,7 @@ struct ts_ctx {
     ts::DevBuf order;              // the order of the last sort_by_key
     ts::DevBuf meta;               // scan state, plan, histograms, scans, counters, carries
     ts::DevBuf lookback;           // two look-back regions
+    ts::DevBuf runs;               // a diverted sort's list of long runs
     ts::DevBuf gather;             // apply_order staging
     ts::DevBuf seg;                // segmented sort: plan, work counter, bin lists, offsets
     ts::DevBuf learn;              // learned partition: sample, model, training state, bucket counts
@@ -52,8 +53,8 @@ struct ts_ctx {
     // plain device sort: the launch sequence of a repeated call, captured on
     // its second identical call and replayed afterwards
     cudaGraphExec_t sort_graph = nullptr;
-    size_t sort_graph_key[8] = {};
-    size_t sort_last_key[8] = {};
+    size_t sort_graph_key[9] = {};
+    size_t sort_last_key[9] = {};
     unsigned long long sort_graph_launches = 0;
 
     // host-slice sorts of at least transfer_min_bytes cross as transfer_chunks
@@ -68,6 +69,9 @@ struct ts_ctx {
     void* stage = nullptr;                 // pinned host memory: STAGE_SLOTS slots
     std::vector<cudaEvent_t> stage_events; // the last DMA of each slot
     ts::CopyPool* copy_pool = nullptr;
+
+    // the tier of the last plain sort (ts_sort_info: 1 small, 2 counting, 3 LSD)
+    int last_tier = 0;
 
     std::string last_error;
     unsigned long long launches = 0;   // kernels this context has launched

@@ -14,6 +14,7 @@
 #include <type_traits>
 
 #include "ts_ctx.h"
+#include "ts_divert.cuh"
 #include "ts_lsd.cuh"
 #include "ts_onesweep.cuh"
 #include "ts_small.cuh"
@@ -29,6 +30,10 @@ struct LsdCfg {
     // the first live pass of a keys-only sort ranks with shared atomics
     // (k_onesweep, UNSTABLE1)
     static constexpr bool UNSTABLE1 = true;
+    // 8-byte keys without positions divert (src/radix/divert.rs): k_plan may
+    // leave out the lowest live digits, and k_divert_runs / k_divert_long
+    // finish the runs that leaves
+    static constexpr bool DIVERT = !PAIRS && sizeof(U) == 8;
     // the largest tile for which two CTAs (one tile of keys and positions, the
     // staging tile, 32-bit per-warp counters) share one SM's shared memory:
     // the per-tile costs (look-back, counter scans) shrink per key as tiles
@@ -70,7 +75,11 @@ struct MetaLayout {
         return m;
     }
     size_t zero_bytes() const { return bins_off; }  // scan state .. histograms
+    // in the (zeroed) plan area, after the Plan: the diverted sort's count of
+    // listed runs (u64) and its work counter (u32)
+    size_t divert_off() const { return plan_off + 128; }
 };
+static_assert(sizeof(Plan) <= 128, "the plan area holds the Plan and the divert counters");
 
 // Resident CTAs per SM for `kernel`, raising its dynamic shared memory limit
 // first when it needs more than the default 48 KB. Cached per kernel.
@@ -126,7 +135,7 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         ++c->launches;
     }
     mark(c, "plan");
-    k_plan<U, XF, C::BITS><<<1, 1024, 0, c->stream>>>(in, n, st, hist, bins, plan, PAIRS ? 1 : 0);
+    k_plan<U, XF, C::BITS, C::DIVERT><<<1, 1024, 0, c->stream>>>(in, n, st, hist, bins, plan, PAIRS ? 1 : 0);
     ++c->launches;
     {
         using Sm = typename C::Smem;
@@ -187,8 +196,9 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
             const size_t work = (n + 15) / 16;
             const int grid = (int)std::min((work + 255) / 256, (size_t)c->sm_count * 8);
             k_fill8<XF><<<grid, 256, 0, c->stream>>>((uint8_t*)d_data, n, h);
-        ++c->launches;
+            ++c->launches;
             mark(c, "end");
+            c->last_tier = 2;
             return TS_OK;
         }
     }
@@ -198,13 +208,22 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         k_small_sort<U, XF, false><<<1, threads, 0, c->stream>>>(d_data, d_data, nullptr, (int)n, 1);
         ++c->launches;
         mark(c, "end");
+        c->last_tier = 1;
         return TS_OK;
     }
     if constexpr (sizeof(U) > 1) {
+        c->last_tier = 3;
         ts_status s;
         if (!d_alt) {
             if ((s = grow(c, c->alt, n * sizeof(U), "scratch keys")) != TS_OK) return s;
             d_alt = (U*)c->alt.p;
+        }
+        constexpr bool DIVERT = LsdCfg<U, false>::DIVERT;
+        // a diverted sort lists the starts of its runs longer than DIVERT_SHORT
+        const size_t runs_cap = n / (DIVERT_SHORT + 1) + 1;
+        if constexpr (DIVERT) {
+            if ((s = grow(c, c->runs, runs_cap * 8, "divert runs")) != TS_OK) return s;
+            occupancy_of((const void*)k_divert_long<U, XF>, SEG_THREADS, MSD_SMEM);
         }
         auto enqueue = [&]() -> ts_status {
             Plan* plan = nullptr;
@@ -215,6 +234,18 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
             const int grid = c->sm_count * 4;
             k_finish_keys<U><<<grid, 512, 0, c->stream>>>(plan, d_alt, d_data, n, aligned16(d_alt) && aligned16(d_data));
             ++c->launches;
+            if constexpr (DIVERT) {
+                const MetaLayout m = MetaLayout::make(LsdCfg<U, false>::ND, LsdCfg<U, false>::RADIX, 0);
+                char* dv = (char*)c->meta.p + m.divert_off();
+                unsigned long long* n_runs = (unsigned long long*)dv;
+                unsigned int* counter = (unsigned int*)(dv + 8);
+                mark(c, "divert");
+                k_divert_runs<U, XF><<<c->sm_count * 8, 256, 0, c->stream>>>(
+                    plan, d_data, n, (unsigned long long*)c->runs.p, n_runs, runs_cap, c->d_error);
+                k_divert_long<U, XF><<<c->sm_count, SEG_THREADS, MSD_SMEM, c->stream>>>(
+                    plan, d_data, d_alt, n, (const unsigned long long*)c->runs.p, n_runs, counter, c->d_error);
+                c->launches += 2;
+            }
             mark(c, "end");
             return TS_OK;
         };
@@ -225,8 +256,8 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         if (c->stream) cudaStreamIsCapturing(c->stream, &cs);
         if (!c->use_graphs || !c->stream || c->timing || cs != cudaStreamCaptureStatusNone) return enqueue();
-        const size_t key[8] = {sizeof(U) * 4 + (size_t)XF, (size_t)d_data, (size_t)d_alt, n, (size_t)c->meta.p,
-                               (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p};
+        const size_t key[9] = {sizeof(U) * 4 + (size_t)XF, (size_t)d_data, (size_t)d_alt, n, (size_t)c->meta.p,
+                               (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p, (size_t)c->runs.p};
         if (c->sort_graph && std::memcmp(key, c->sort_graph_key, sizeof key) == 0) {
             TS_CUDA(c, cudaGraphLaunch(c->sort_graph, c->stream));
             c->launches += c->sort_graph_launches;

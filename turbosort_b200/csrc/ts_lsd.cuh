@@ -209,12 +209,44 @@ __global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, siz
 }
 
 // ---------------------------------------------------------------------------
+// Diverting (src/radix/divert.rs:38-54, :95-104): how many of the lowest
+// live digits need no pass, because the digits above them already split the
+// keys into runs short enough to finish by a direct sort of each run.
+// ---------------------------------------------------------------------------
+constexpr int DIVERT_SLACK_BITS = 2;  // divert.rs:19
+constexpr int DIVERT_MIN_SKIP = 3;    // divert.rs:28
+
+// log2(x) in eighths of a bit, never above the true value (divert.rs:95-104)
+__host__ __device__ inline unsigned log2_eighths(unsigned long long x) {
+    int ip = 63;
+    while (ip > 0 && !((x >> ip) & 1ull)) --ip;
+    const unsigned long long frac = ip >= 3 ? (x >> (ip - 3)) & 7ull : (x << (3 - ip)) & 7ull;
+    return 8u * (unsigned)ip + (unsigned)frac;
+}
+
+// max_bucket[i]: the largest bucket of the i-th live digit, least significant first
+__host__ __device__ inline int skippable_digits(int n_live, unsigned long long len,
+                                                const unsigned long long* max_bucket) {
+    const unsigned log_len = log2_eighths(len);
+    const unsigned need = log_len + 8u * DIVERT_SLACK_BITS;
+    unsigned have = 0;
+    for (int i = n_live - 1; i >= DIVERT_MIN_SKIP; --i) {
+        have += log_len - log2_eighths(max_bucket[i]);
+        if (have >= need) return i;
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
 // k_plan: one CTA. Live passes are the counted digits whose histogram does
 // not hold every key in the first key's bucket; each gets its exclusive scan.
 // `stable` (sort_by_key) leaves descending input to the passes, since a
-// plain reversal would reverse equal keys.
+// plain reversal would reverse equal keys. With DIVERT (keys only) the
+// lowest live digits are left out when diverting.rs's rule allows it
+// (src/radix/mod.rs:240-242), and divert_shift tells the finishing kernels
+// which runs remain.
 // ---------------------------------------------------------------------------
-template <typename U, int XF, int BITS>
+template <typename U, int XF, int BITS, bool DIVERT = false>
 __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
                                                const unsigned long long* __restrict__ ghist,
                                                unsigned long long* __restrict__ bins, Plan* __restrict__ plan,
@@ -222,6 +254,7 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
     __shared__ int live_s[ND];
+    __shared__ unsigned long long max_s[ND];
     const U first = to_key<U, XF>(src[0]);
     const unsigned long long diff = st->diff;
     if (threadIdx.x < ND) {
@@ -233,10 +266,11 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
     // warp w scans digit w's histogram
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp < ND && live_s[warp]) {
-        unsigned long long carry = 0;
+        unsigned long long carry = 0, mx = 0;
         for (int r0 = 0; r0 < RADIX; r0 += 32) {
             const int r = r0 + lane;
             unsigned long long v = r < RADIX ? ghist[(size_t)warp * RADIX + r] : 0ull;
+            mx = v > mx ? v : mx;
             unsigned long long x = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -246,17 +280,35 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
             if (r < RADIX) bins[(size_t)warp * RADIX + r] = carry + x - v;
             carry += __shfl_sync(0xffffffffu, x, 31);
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long y = __shfl_xor_sync(0xffffffffu, mx, o);
+            mx = y > mx ? y : mx;
+        }
+        if (lane == 0) max_s[warp] = mx;
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned f = st->flags;
         int mode = MODE_SORT;
         if (!(f & SCAN_NOT_ASC)) mode = MODE_SORTED;
         else if (!stable && !(f & SCAN_NOT_DESC)) mode = MODE_REVERSE;
+        int live[ND];
+        unsigned long long maxb[ND];
         int m = 0;
         if (mode == MODE_SORT)
             for (int d = 0; d < ND; ++d)
-                if (live_s[d]) plan->pass[m++] = d;
-        plan->n_live = m;
+                if (live_s[d]) {
+                    maxb[m] = max_s[d];
+                    live[m++] = d;
+                }
+        int skip = 0;
+        if constexpr (DIVERT) {
+            if (!stable && mode == MODE_SORT) skip = skippable_digits(m, n, maxb);
+        }
+        for (int i = skip; i < m; ++i) plan->pass[i - skip] = live[i];
+        plan->n_live = m - skip;
+        plan->divert_shift = skip > 0 ? live[skip] * BITS : 0;
         plan->mode = mode;
     }
 }
