@@ -100,6 +100,14 @@ typedef struct ts_sort_info {
 } ts_sort_info;
 ts_status ts_ctx_last_sort_info(ts_ctx *ctx, ts_sort_info *info);
 
+/* Test hook for failure detection, no counterpart in the crate: in the next
+ * LSD sort on this context (keys or order, more than 4096 keys), the first
+ * scatter pass's tile 0 never publishes its look-back entry, and every wait
+ * on it gives up after spin_limit rounds (normally about a million). The
+ * sort then reports TS_ERR_TIMEOUT with every write kept inside the output
+ * and scratch buffers; the context stays usable. 0 disarms it. */
+ts_status ts_ctx_test_stall_lookback(ts_ctx *ctx, uint32_t spin_limit);
+
 /* The diverting rule of the crate (src/radix/divert.rs:38-54) as the device
  * applies it: how many of the lowest of n_live live digits need no pass, for
  * len keys whose i-th live digit (least significant first) has its largest

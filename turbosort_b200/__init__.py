@@ -167,6 +167,8 @@ def lib() -> ctypes.CDLL:
             L.ts_ctx_launches.restype = ctypes.c_ulonglong
             L.ts_ctx_last_sort_info.argtypes = [vp, ctypes.POINTER(SortInfo)]
             L.ts_ctx_last_sort_info.restype = st
+            L.ts_ctx_test_stall_lookback.argtypes = [vp, ctypes.c_uint32]
+            L.ts_ctx_test_stall_lookback.restype = st
             L.ts_divert_skippable_digits.argtypes = [i, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
             L.ts_divert_skippable_digits.restype = i
             L.ts_apply_order.argtypes = [vp, vp, sz, sz, vp, sz]

@@ -424,6 +424,12 @@ ts_status ts_ctx_last_sort_info(ts_ctx* c, ts_sort_info* info) {
     return TS_OK;
 }
 
+ts_status ts_ctx_test_stall_lookback(ts_ctx* c, uint32_t spin_limit) {
+    if (!c) return TS_ERR_INVALID;
+    c->test_spin_limit = spin_limit;
+    return TS_OK;
+}
+
 int ts_divert_skippable_digits(int n_live, uint64_t len, const uint64_t* max_bucket) {
     if (n_live <= 0 || len == 0 || !max_bucket) return 0;
     return skippable_digits(n_live, (unsigned long long)len, (const unsigned long long*)max_bucket);

@@ -70,6 +70,9 @@ struct ts_ctx {
     std::vector<cudaEvent_t> stage_events; // the last DMA of each slot
     ts::CopyPool* copy_pool = nullptr;
 
+    // test hook (ts_ctx_test_stall_lookback): the next LSD sort's first pass
+    // withholds tile 0's look-back entry and gives up after this many rounds
+    uint32_t test_spin_limit = 0;
     // the tier of the last plain sort (ts_sort_info: 1 small, 2 counting, 3 LSD)
     int last_tier = 0;
 

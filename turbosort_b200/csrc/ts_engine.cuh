@@ -157,6 +157,7 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         a.plan = plan;
         a.bins = bins;
         a.error = c->d_error;
+        a.spin_limit = c->test_spin_limit ? c->test_spin_limit : SPIN_LIMIT;
         int launch = 0;
         for (int slot = 0; slot < ND; ++slot) {
             for (int q = 0; q < portions; ++q, ++launch) {
@@ -169,6 +170,7 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
                 a.lookback_next = lb + (size_t)((launch + 1) & 1) * lb_words;
                 a.lookback_words = lb_words;
                 a.tile_counter = counters + launch;
+                a.withhold_tile0 = c->test_spin_limit != 0 && launch == 0;
                 const int grid = (int)std::min((size_t)c->sm_count * occ, (size_t)a.portion_tiles);
                 mark(c, "onesweep");
                 kern<<<grid, C::THREADS, Sm::bytes, c->stream>>>(a);
@@ -176,6 +178,7 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
             }
         }
     }
+    c->test_spin_limit = 0;  // the test hook covers one sort
     *plan_out = plan;
     return TS_OK;
 }
@@ -255,7 +258,8 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         // while per-kernel timing is on, nor inside the caller's own capture.
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         if (c->stream) cudaStreamIsCapturing(c->stream, &cs);
-        if (!c->use_graphs || !c->stream || c->timing || cs != cudaStreamCaptureStatusNone) return enqueue();
+        if (!c->use_graphs || !c->stream || c->timing || c->test_spin_limit || cs != cudaStreamCaptureStatusNone)
+            return enqueue();
         const size_t key[9] = {sizeof(U) * 4 + (size_t)XF, (size_t)d_data, (size_t)d_alt, n, (size_t)c->meta.p,
                                (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p, (size_t)c->runs.p};
         if (c->sort_graph && std::memcmp(key, c->sort_graph_key, sizeof key) == 0) {

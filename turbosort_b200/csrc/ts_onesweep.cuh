@@ -49,6 +49,8 @@ struct SweepArgs {
     size_t lookback_words;       // words per region (a multiple of 4)
     uint32_t* tile_counter;      // zeroed before the launch
     uint32_t* error;
+    uint32_t spin_limit;         // look-back rounds without progress before ERR_TIMEOUT
+    int withhold_tile0;          // test hook: tile 0 never publishes (its successors' waits run out)
 };
 
 template <typename U, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF>
@@ -280,7 +282,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                 }
                 tcount[q] = s;
                 own += s;
-                st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, (t == 0 ? LB_FLAG_INC : LB_FLAG_AGG) | s);
+                if (t != 0 || !a.withhold_tile0)
+                    st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, (t == 0 ? LB_FLAG_INC : LB_FLAG_AGG) | s);
             }
         }
         uint32_t x = own;
@@ -375,7 +378,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                             if (f == LB_FLAG_INC) done = true;
                         }
                         j -= adv;
-                        if (adv == 0 && ++spins > SPIN_LIMIT) {
+                        if (adv == 0 && ++spins > a.spin_limit) {
                             atomicOr(a.error, ERR_TIMEOUT);
                             break;
                         }
