@@ -4,7 +4,8 @@
 // When k_plan diverts, the passes sort only the digits from divert_shift up:
 // the keys then come out ordered by that prefix, in runs of keys sharing it
 // (most runs one key long), and each run only needs sorting within itself.
-//   k_divert_runs  one read of the keys, 32 consecutive keys a warp: a key
+//   k_divert_runs  one read of the keys, 16-byte loads, 32 * KPT consecutive
+//                  keys a warp step: a key
 //                  whose prefix differs from its predecessor's and equals its
 //                  successor's starts a run of two or more. Its thread finds
 //                  the run's end (galloping, then bisecting, over the sorted
@@ -55,53 +56,103 @@ __device__ size_t divert_run_end(const U* d, size_t n, size_t s, int shift) {
     return hi;
 }
 
+// The run starting at s (len keys, 2 <= len <= DIVERT_SHORT) sorted in place.
+template <typename U, int XF>
+__device__ void divert_sort_short(U* d, size_t s, size_t len) {
+    if (len == 2) {  // most runs: two keys, kept in registers
+        const U a = d[s], b = d[s + 1];
+        if (to_key<U, XF>(a) > to_key<U, XF>(b)) {
+            d[s] = b;
+            d[s + 1] = a;
+        }
+        return;
+    }
+    U k[DIVERT_SHORT];
+    for (size_t j = 0; j < len; ++j) k[j] = to_key<U, XF>(d[s + j]);
+    bool moved = false;
+    for (size_t j = 1; j < len; ++j) {
+        const U x = k[j];
+        size_t q = j;
+        while (q > 0 && k[q - 1] > x) {
+            k[q] = k[q - 1];
+            --q;
+        }
+        k[q] = x;
+        moved |= q != j;
+    }
+    if (moved)
+        for (size_t j = 0; j < len; ++j) d[s + j] = from_key<U, XF>(k[j]);
+}
+
+// KPT keys a lane, consecutive (16-byte loads when the keys are aligned),
+// a warp 32 * KPT consecutive keys per step, two steps' loads in flight.
 template <typename U, int XF>
 __global__ void __launch_bounds__(256) k_divert_runs(const Plan* __restrict__ plan, U* d, size_t n,
                                                      unsigned long long* __restrict__ runs,
                                                      unsigned long long* __restrict__ n_runs, size_t runs_cap,
-                                                     uint32_t* __restrict__ error) {
+                                                     uint32_t* __restrict__ error, int vec_ok) {
     if (plan->mode != MODE_SORT || plan->divert_shift <= 0) return;
+    constexpr int KPT = 32 / sizeof(U);  // two 16-byte vectors
+    constexpr int W = 32 * KPT;          // keys a warp step
     const int shift = plan->divert_shift;
     auto pre = [&](U v) { return (unsigned long long)to_key<U, XF>(v) >> shift; };
     const int lane = threadIdx.x & 31;
     const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
-    for (size_t wb = gw * 32; wb < n; wb += nw * 32) {  // warp-uniform
-        const size_t i = wb + lane;
-        const bool valid = i < n;
-        const U v = valid ? d[i] : (U)0;
-        U prev = __shfl_up_sync(0xffffffffu, v, 1);
-        U next = __shfl_down_sync(0xffffffffu, v, 1);
-        if (lane == 0 && valid && i > 0) prev = d[i - 1];
-        if (lane == 31 && i + 1 < n) next = d[i + 1];
-        if (!valid) continue;
-        const unsigned long long p = pre(v);
-        const bool start = i == 0 || pre(prev) != p;
-        if (!start || i + 1 >= n || pre(next) != p) continue;
-        // a run of two or more keys starts here
-        const size_t e = divert_run_end<U, XF>(d, n, i, shift);
-        const size_t len = e - i;
-        if (len <= (size_t)DIVERT_SHORT) {
-            U k[DIVERT_SHORT];
-            for (size_t j = 0; j < len; ++j) k[j] = to_key<U, XF>(d[i + j]);
-            bool moved = false;
-            for (size_t j = 1; j < len; ++j) {
-                const U x = k[j];
-                size_t q = j;
-                while (q > 0 && k[q - 1] > x) {
-                    k[q] = k[q - 1];
-                    --q;
-                }
-                k[q] = x;
-                moved |= q != j;
-            }
-            if (moved)
-                for (size_t j = 0; j < len; ++j) d[i + j] = from_key<U, XF>(k[j]);
+    auto load = [&](size_t base, U (&k)[KPT]) {
+        const size_t i0 = base + (size_t)lane * KPT;
+        if (vec_ok && i0 + KPT <= n) {
+            const uint4* p = reinterpret_cast<const uint4*>(d + i0);
+            union {
+                uint4 q[2];
+                U e[KPT];
+            } u;
+            u.q[0] = p[0];
+            u.q[1] = p[1];
+#pragma unroll
+            for (int e = 0; e < KPT; ++e) k[e] = u.e[e];
         } else {
-            const unsigned long long slot = atomicAdd(n_runs, 1ull);
-            if (slot < runs_cap) runs[slot] = i;
-            else atomicOr(error, ERR_BOUNDS);  // cannot happen: a listed run holds more than DIVERT_SHORT keys
+#pragma unroll
+            for (int e = 0; e < KPT; ++e) k[e] = i0 + e < n ? d[i0 + e] : (U)0;
         }
+    };
+    auto step = [&](size_t base, const U (&k)[KPT]) {
+        const size_t i0 = base + (size_t)lane * KPT;
+        U prev = __shfl_up_sync(0xffffffffu, k[KPT - 1], 1);
+        U next = __shfl_down_sync(0xffffffffu, k[0], 1);
+        if (lane == 0 && i0 > 0 && i0 < n) prev = d[i0 - 1];
+        if (lane == 31 && i0 + KPT < n) next = d[i0 + KPT];
+        unsigned long long pp = pre(prev);
+#pragma unroll
+        for (int e = 0; e < KPT; ++e) {
+            const size_t i = i0 + e;
+            if (i >= n) break;
+            const unsigned long long p = pre(k[e]);
+            const bool start = i == 0 || pp != p;
+            pp = p;
+            if (!start || i + 1 >= n) continue;
+            const unsigned long long pn = pre(e + 1 < KPT ? k[e + 1] : next);
+            if (pn != p) continue;
+            // a run of two or more keys starts here
+            const size_t end = divert_run_end<U, XF>(d, n, i, shift);
+            const size_t len = end - i;
+            if (len <= (size_t)DIVERT_SHORT) {
+                divert_sort_short<U, XF>(d, i, len);
+            } else {
+                const unsigned long long slot = atomicAdd(n_runs, 1ull);
+                if (slot < runs_cap) runs[slot] = i;
+                else atomicOr(error, ERR_BOUNDS);  // cannot happen: a listed run holds more than DIVERT_SHORT keys
+            }
+        }
+    };
+    for (size_t wb = gw * W; wb < n; wb += 2 * nw * W) {  // warp-uniform
+        U a[KPT], b[KPT];
+        load(wb, a);
+        const size_t wb2 = wb + nw * W;
+        const bool two = wb2 < n;  // warp-uniform
+        if (two) load(wb2, b);
+        step(wb, a);
+        if (two) step(wb2, b);
     }
 }
 

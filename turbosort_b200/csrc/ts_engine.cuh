@@ -2,8 +2,9 @@
 //
 // The tier choice follows the crate's dispatcher (src/dispatch.rs:31-111):
 // n <= 1 is a no-op; one-byte keys take the counting sort
-// (src/radix/mod.rs:123-164); short slices take the bitonic tier
-// (src/tiny.rs, src/small.rs, here up to 4096 keys); the rest runs the LSD
+// (src/radix/mod.rs:123-164); short slices take the bitonic tiers
+// (src/tiny.rs, src/small.rs: one warp in registers up to 256 keys, one CTA
+// in shared memory up to 4096); the rest runs the LSD
 // passes (src/radix/mod.rs:180-271). The presorted early-out
 // (src/presorted.rs:15-65) and the constant-digit skip are decided on the
 // device, so nothing in a sort waits on the host.
@@ -42,10 +43,13 @@ struct LsdCfg {
     static constexpr int IPT = sizeof(U) == 8 ? (PAIRS ? 7 : 11) : (PAIRS ? 11 : (sizeof(U) == 4 ? 22 : 32));
     static constexpr int NBUF = 1;  // tiles of keys in flight per CTA; the next one is prefetched into L2
     // items with i % MATCH_MOD < MATCH_CNT find their digit's peers with
-    // match.any, the rest with ballots: one item in four keeps the match unit
-    // busy without making it the bottleneck and takes a quarter of the ranking
-    // off the integer pipe (2^28 u32 keys on a B200: 5.81 -> 5.19 ms a sort)
-    static constexpr int MATCH_MOD = 4;
+    // match.any, the rest with ballots: a share of the items keeps the match
+    // unit busy without making it the bottleneck and takes that share of the
+    // ranking off the integer pipe (2^28 u32 keys on a B200, one in four:
+    // 5.81 -> 5.19 ms a sort; with the unstable first pass, u32 one in three
+    // 4.32 ms, one in four 4.34, one in five 4.41; u64 one in four 6.58, one
+    // in three 6.71)
+    static constexpr int MATCH_MOD = (sizeof(U) == 8 || PAIRS) ? 4 : 3;
     static constexpr int MATCH_CNT = 1;
     using Smem = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
     static constexpr int TILE = Smem::TILE;
@@ -207,8 +211,14 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
     }
     if (n <= (size_t)SMALL_MAX) {
         mark(c, "small");
-        const int threads = (int)std::min<size_t>(SMALL_THREADS, std::max<size_t>(32, (n + 1) / 2));
-        k_small_sort<U, XF, false><<<1, threads, 0, c->stream>>>(d_data, d_data, nullptr, (int)n, 1);
+        if (n <= 32) {
+            k_warp_sort<U, XF, 1><<<1, 32, 0, c->stream>>>(d_data, (int)n);
+        } else if (n <= (size_t)WARP_TIER_MAX) {
+            k_warp_sort<U, XF, WARP_TIER_MAX / 32><<<1, 32, 0, c->stream>>>(d_data, (int)n);
+        } else {
+            const int threads = (int)std::min<size_t>(SMALL_THREADS, std::max<size_t>(32, (n + 1) / 2));
+            k_small_sort<U, XF, false><<<1, threads, 0, c->stream>>>(d_data, d_data, nullptr, (int)n, 1);
+        }
         ++c->launches;
         mark(c, "end");
         c->last_tier = 1;
@@ -244,7 +254,7 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
                 unsigned int* counter = (unsigned int*)(dv + 8);
                 mark(c, "divert");
                 k_divert_runs<U, XF><<<c->sm_count * 8, 256, 0, c->stream>>>(
-                    plan, d_data, n, (unsigned long long*)c->runs.p, n_runs, runs_cap, c->d_error);
+                    plan, d_data, n, (unsigned long long*)c->runs.p, n_runs, runs_cap, c->d_error, aligned16(d_data));
                 k_divert_long<U, XF><<<c->sm_count, SEG_THREADS, MSD_SMEM, c->stream>>>(
                     plan, d_data, d_alt, n, (const unsigned long long*)c->runs.p, n_runs, counter, c->d_error);
                 c->launches += 2;

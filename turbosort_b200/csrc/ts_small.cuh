@@ -1,5 +1,7 @@
 // ts_small.cuh — the short-slice tiers and the one-byte counting sort.
 //
+//   k_warp_sort    one warp sorts up to 32 or WARP_TIER_MAX keys in registers
+//                  (bitonic: shuffles between lanes, swaps inside a lane)
 //   k_small_sort   one CTA sorts up to SMALL_MAX keys with a bitonic network
 //                  in shared memory, padding with the largest key exactly as
 //                  the crate's AVX2 networks pad with u32::MAX
@@ -16,6 +18,7 @@
 namespace ts {
 
 constexpr int SMALL_MAX = 4096;
+constexpr int WARP_TIER_MAX = 256;  // k_warp_sort with 8 keys a lane
 constexpr int SMALL_THREADS = 1024;
 
 // `in` and `out` may be the same array (the keys are all in shared memory
@@ -59,6 +62,59 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small_sort(const U* in, U* ou
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         if (write_keys) out[i] = from_key<U, XF>(sk[i]);
         if constexpr (PAIRS) order[i] = sv[i];
+    }
+}
+
+// One warp sorts up to 32 * R keys in registers: element e = r * 32 + lane
+// sits in register r of that lane. A bitonic network over the next power of
+// two, padded with the largest key as the crate's AVX2 tiers pad
+// (src/arch/x86_64/avx2.rs:211-313): partners 32 and more apart are in the
+// same lane (a register swap), closer ones in another lane (a shuffle). No
+// shared memory and no block barrier: the tier for the slices the crate
+// sends to its register networks (src/tiny.rs:15, src/small.rs:11).
+template <typename U, int XF, int R>
+__global__ void __launch_bounds__(32) k_warp_sort(U* d, int n) {
+    constexpr int N = 32 * R;
+    const int lane = threadIdx.x;
+    U v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int e = r * 32 + lane;
+        v[r] = e < n ? to_key<U, XF>(d[e]) : (U)~(U)0;
+    }
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int rp = r ^ (j >> 5);
+                    if (rp > r) {
+                        const bool up = ((r * 32) & k) == 0;
+                        const U a = v[r], b = v[rp];
+                        const bool sw = (a > b) == up;
+                        v[r] = sw ? b : a;
+                        v[rp] = sw ? a : b;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int e = r * 32 + lane;
+                    const U o = __shfl_xor_sync(0xffffffffu, v[r], j);
+                    const bool up = (e & k) == 0;
+                    const bool lower = (e & j) == 0;
+                    const bool keep_min = lower == up;
+                    v[r] = keep_min ? (o < v[r] ? o : v[r]) : (o > v[r] ? o : v[r]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int e = r * 32 + lane;
+        if (e < n) d[e] = from_key<U, XF>(v[r]);
     }
 }
 
