@@ -212,6 +212,13 @@ typedef struct ts_learned_params {
     int32_t use_model;       /* 0: equal-width buckets (ablation) */
     uint64_t corrupt_seed;   /* test hook, 0 = off: overwrite the trained leaves with
                                 arbitrary values before the partition (output stays exact) */
+    uint32_t route_passes;   /* cost route: when the plain sort would need at most this many
+                                scatter passes (estimated from the sample's digit histograms,
+                                diverting included; keys of at most this many bytes need no
+                                estimate), the plain sort runs instead (reason 4); 0 = never */
+    int32_t verify;          /* the judge: 1 = sort a copy with the plain LSD as well and count
+                                the keys where the outputs differ (stats->verify_mismatches);
+                                any difference returns TS_ERR_INTERNAL */
 } ts_learned_params;
 
 typedef struct ts_learned_stats {
@@ -221,8 +228,14 @@ typedef struct ts_learned_stats {
     float max_cdf_error;
     uint32_t train_iters;
     int32_t fell_back;  /* 1: the plain sort produced the output */
-    int32_t reason;     /* 1 bucket overflow, 2 CDF error, 3 input below 2^20 keys */
+    int32_t reason;     /* 1 bucket overflow, 2 CDF error, 3 input below 2^20 keys,
+                           4 routed: the plain sort's estimated passes <= route_passes */
     float ms_sample, ms_train, ms_partition, ms_buckets;
+    int32_t est_plain_passes;     /* the plain sort's estimated scatter passes (-1: not estimated) */
+    int32_t verified;             /* 1: the judge compared the output with the plain sort's */
+    uint64_t verify_mismatches;   /* keys where they differ (0 when correct) */
+    float ms_verify;
+    float pad;
 } ts_learned_stats;
 
 void ts_learned_defaults(ts_learned_params *params);

@@ -13,11 +13,28 @@ pytestmark = pytest.mark.gpu
 N = 1 << 21  # above the learned path's 2^20-key floor; the oracle sorts it in well under a second
 
 
+class _PartitionUnderTest:
+    """The package, with the learned sort's cost route off unless a test sets
+    it: these tests are about the partition itself, which the route would
+    skip for 4-byte keys and for keys the plain sort diverts."""
+
+    def __init__(self, ts):
+        self._ts = ts
+
+    def __getattr__(self, name):
+        return getattr(self._ts, name)
+
+    def sort_learned(self, a, params=None, ctx=None, **overrides):
+        if params is None:
+            overrides.setdefault("route_passes", 0)
+        return self._ts.sort_learned(a, params, ctx, **overrides)
+
+
 @pytest.fixture(scope="module")
 def ts():
     import turbosort_b200 as ts
 
-    return ts
+    return _PartitionUnderTest(ts)
 
 
 @pytest.fixture(scope="module")
@@ -269,3 +286,37 @@ def test_full_size_equals_plain_sort(ts, W):
     torch.cuda.synchronize()
     assert st["fell_back"] == 0, st
     assert torch.equal(a.view(torch.int64), b.view(torch.int64))
+
+
+@pytest.mark.parametrize("kind, routed", [("unit_f32_dups", True), ("uniform_u32", True), ("uniform_u64", True),
+                                          ("lognormal_f64", False), ("gauss_mix_u64", False)])
+def test_cost_route(ts, W, kind, routed):
+    """With the default route, inputs the plain sort handles in at most five
+    passes (every 4-byte key; random 8-byte keys, which it diverts to four)
+    take the plain sort; skewed 8-byte keys that need all eight passes take
+    the partition. The output is the oracle's either way."""
+    import turbosort_b200 as real
+
+    a = inputs(W, kind)
+    got = a.copy()
+    st = real.sort_learned(got)
+    same_bits(got, O.sort(a))
+    if routed:
+        assert st["fell_back"] == 1 and st["reason"] == 4, st
+        assert 0 < st["est_plain_passes"] <= 5, st
+    else:
+        assert st["reason"] != 4 and st["est_plain_passes"] >= 6, st
+
+
+@pytest.mark.parametrize("kind", ["lognormal_f64", "gauss_mix_u64", "unit_f32_dups", "specials_f64"])
+def test_judge_compares_with_the_plain_sort(ts, W, kind):
+    """verify = 1: the plain LSD sorts a copy on the device and the outputs
+    are compared key for key; a good model and a corrupted one both agree."""
+    a = inputs(W, kind, seed=33)
+    want = O.sort(a)
+    for extra in ({}, {"corrupt_seed": 5, "overflow_factor": 1e9, "max_cdf_error": 1e9}):
+        got = a.copy()
+        st = ts.sort_learned(got, verify=1, **extra)
+        same_bits(got, want)
+        if st["fell_back"] == 0:
+            assert st["verified"] == 1 and st["verify_mismatches"] == 0, st

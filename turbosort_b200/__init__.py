@@ -61,7 +61,8 @@ class LearnedParams(ctypes.Structure):
     fallback thresholds of the learned-partition sort."""
     _fields_ = [("buckets_log2", ctypes.c_uint32), ("sample_every", ctypes.c_uint32), ("leaves", ctypes.c_uint32),
                 ("train_iters", ctypes.c_uint32), ("lr", ctypes.c_float), ("overflow_factor", ctypes.c_float),
-                ("max_cdf_error", ctypes.c_float), ("use_model", ctypes.c_int32), ("corrupt_seed", ctypes.c_uint64)]
+                ("max_cdf_error", ctypes.c_float), ("use_model", ctypes.c_int32), ("corrupt_seed", ctypes.c_uint64),
+                ("route_passes", ctypes.c_uint32), ("verify", ctypes.c_int32)]
 
 
 class LearnedStats(ctypes.Structure):
@@ -71,7 +72,9 @@ class LearnedStats(ctypes.Structure):
                 ("train_loss_first", ctypes.c_double), ("train_loss_last", ctypes.c_double),
                 ("max_cdf_error", ctypes.c_float), ("train_iters", ctypes.c_uint32), ("fell_back", ctypes.c_int32),
                 ("reason", ctypes.c_int32), ("ms_sample", ctypes.c_float), ("ms_train", ctypes.c_float),
-                ("ms_partition", ctypes.c_float), ("ms_buckets", ctypes.c_float)]
+                ("ms_partition", ctypes.c_float), ("ms_buckets", ctypes.c_float),
+                ("est_plain_passes", ctypes.c_int32), ("verified", ctypes.c_int32),
+                ("verify_mismatches", ctypes.c_uint64), ("ms_verify", ctypes.c_float), ("pad", ctypes.c_float)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

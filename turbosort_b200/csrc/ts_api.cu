@@ -286,7 +286,7 @@ void ts_ctx_destroy(ts_ctx* c) {
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     if (c->out_stream) cudaStreamSynchronize(c->out_stream);
     for (DevBuf* b : {&c->keys, &c->alt, &c->vals0, &c->vals1, &c->order, &c->meta, &c->lookback, &c->runs, &c->gather,
-                      &c->seg,
+                      &c->seg, &c->check,
                       &c->learn, &c->pipe, &c->pipe_pos[0], &c->pipe_pos[1]})
         if (b->p) cudaFree(b->p);
     for (auto ev : c->pipe_events) cudaEventDestroy(ev);

@@ -82,6 +82,8 @@ struct MetaLayout {
     // in the (zeroed) plan area, after the Plan: the diverted sort's count of
     // listed runs (u64) and its work counter (u32)
     size_t divert_off() const { return plan_off + 128; }
+    // after those: the largest bucket of each digit (u64, 0 when not live)
+    size_t maxb_off() const { return plan_off + 144; }
 };
 static_assert(sizeof(Plan) <= 128, "the plan area holds the Plan and the divert counters");
 
@@ -139,7 +141,9 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         ++c->launches;
     }
     mark(c, "plan");
-    k_plan<U, XF, C::BITS, C::DIVERT><<<1, 1024, 0, c->stream>>>(in, n, st, hist, bins, plan, PAIRS ? 1 : 0);
+    static_assert(144 + 8 * ND <= 256, "the plan area holds every digit's largest bucket");
+    k_plan<U, XF, C::BITS, C::DIVERT><<<1, 1024, 0, c->stream>>>(in, n, st, hist, bins, plan, PAIRS ? 1 : 0,
+                                                                 (unsigned long long*)(meta + m.maxb_off()));
     ++c->launches;
     {
         using Sm = typename C::Smem;

@@ -32,6 +32,7 @@ struct LmBuffers {
     LmTables T;
     double* loss;  // [2]: before the first step, after the last
     float* max_err;
+    unsigned long long* mismatches;  // the judge's count
     unsigned long long *totals, *offsets, *max_bucket, *cur1, *cur2;
     unsigned int *tiles_before, *counter;
     size_t bytes;
@@ -53,6 +54,7 @@ LmBuffers lm_layout(char* base, size_t m, size_t key_bytes, int leaves, int buck
     B.T.last = b.take<int>(leaves);
     B.loss = b.take<double>(2);
     B.max_err = b.take<float>(1);
+    B.mismatches = b.take<unsigned long long>(1);
     B.max_bucket = b.take<unsigned long long>(1);
     B.counter = b.take<unsigned int>(1);
     B.totals = b.take<unsigned long long>(buckets);
@@ -65,6 +67,18 @@ LmBuffers lm_layout(char* base, size_t m, size_t key_bytes, int leaves, int buck
 }
 
 }  // namespace
+
+// keys where a and b differ
+template <typename U>
+__global__ void k_lm_compare(const U* __restrict__ a, const U* __restrict__ b, size_t n,
+                             unsigned long long* __restrict__ count) {
+    unsigned long long c = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        c += a[i] != b[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
 
 struct Events {
     cudaEvent_t e[7] = {};
@@ -107,14 +121,29 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
         return done(fail(c, TS_ERR_INVALID, "learned partition: leaves and buckets exceed shared memory"));
     const size_t every = std::max<uint32_t>(2, prm.sample_every);
     const size_t m = n / every;
-    if (n < (1u << 20) || m < 2 * (size_t)leaves) {  // too small for the model to pay
+    const bool too_small = n < (1u << 20) || m < 2 * (size_t)leaves;  // too small for the model to pay
+    const int iters = std::max(0, (int)prm.train_iters);
+    S.est_plain_passes = -1;
+    if (too_small) {
         S.fell_back = 1;
         S.reason = 3;
-        ts_status s = sort_keys_device<U, XF>(c, d, n, nullptr);
-        if (s == TS_OK) s = finish(c);
-        return done(s);
+        ts_status s3 = sort_keys_device<U, XF>(c, d, n, nullptr);
+        if (s3 == TS_OK) s3 = finish(c);
+        return done(s3);
     }
-    const int iters = std::max(0, (int)prm.train_iters);
+    // the cost route: keys of at most route_passes bytes never need more than
+    // that many 8-bit passes, so the plain sort runs without a sample
+    auto plain = [&](int reason) {
+        S.fell_back = 1;
+        S.reason = reason;
+        ts_status s2 = sort_keys_device<U, XF>(c, d, n, nullptr);
+        if (s2 == TS_OK) s2 = finish(c);
+        return done(s2);
+    };
+    if (prm.route_passes > 0 && sizeof(U) <= prm.route_passes) {
+        S.est_plain_passes = (int32_t)sizeof(U);
+        return plain(4);
+    }
 
     ts_status s;
     LmBuffers B = lm_layout(nullptr, m, sizeof(U), leaves, buckets);
@@ -135,6 +164,13 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     TS_CUDA(c, cudaFuncSetAttribute((const void*)k_lm_finish<U, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     MSD_SMEM));
 
+    U* check = nullptr;  // the judge's copy of the input
+    if (prm.verify) {
+        if ((s = grow(c, c->check, n * sizeof(U) + 16, "judge copy")) != TS_OK) return done(s);
+        check = (U*)c->check.p;
+        TS_CUDA(c, cudaMemcpyAsync(check, d, n * sizeof(U), cudaMemcpyDeviceToDevice, c->stream));
+    }
+
     Events ev;
     mark(c, "lm_sample");
     cudaEventRecord(ev.e[0], c->stream);
@@ -143,6 +179,29 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     k_lm_sample<U><<<c->sm_count * 4, 256, 0, c->stream>>>(d, n, every, sample, m, XF);
     ++c->launches;
     if ((s = sort_keys_device<U, 0>(c, sample, m, nullptr)) != TS_OK) return done(s);
+    if (prm.route_passes > 0) {
+        // the sample's digit histograms stand for the input's: its live
+        // digits, and each digit's largest bucket scaled to n keys, give the
+        // passes the plain sort would run (diverting included)
+        constexpr int ND = (int)sizeof(U);
+        unsigned long long maxb[ND];
+        const MetaLayout ml = MetaLayout::make(ND, 256, 0);
+        TS_CUDA(c, cudaMemcpyAsync(maxb, (const char*)c->meta.p + ml.maxb_off(), sizeof maxb, cudaMemcpyDeviceToHost,
+                                   c->stream));
+        TS_CUDA(c, cudaStreamSynchronize(c->stream));
+        unsigned long long scaled[ND];
+        int live = 0;
+        for (int dg = 0; dg < ND; ++dg)
+            if (maxb[dg]) {
+                const double f = (double)maxb[dg] * (double)n / (double)m;
+                scaled[live++] = (unsigned long long)std::min<double>((double)n, std::max(1.0, f));
+            }
+        S.est_plain_passes = live - skippable_digits(live, n, scaled);
+        if (S.est_plain_passes <= (int)prm.route_passes) {
+            S.ms_sample = 0.f;
+            return plain(4);
+        }
+    }
     mark(c, "lm_fit");
     TS_CUDA(c, cudaMemsetAsync(B.T.first, 0xff, (size_t)leaves * 4, c->stream));
     TS_CUDA(c, cudaMemsetAsync(B.T.last, 0xff, (size_t)leaves * 4, c->stream));
@@ -235,7 +294,26 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     ++c->launches;
     TS_CUDA(c, cudaGetLastError());
     cudaEventRecord(ev.e[6], c->stream);
-    s = finish(c);
+    if (check) {
+        // the judge: the plain LSD sorts the copy, and the outputs must agree
+        // key for key (an exact sort has one output)
+        TS_CUDA(c, cudaMemsetAsync(B.mismatches, 0, 8, c->stream));
+        if ((s = sort_keys_device<U, XF>(c, check, n, nullptr)) != TS_OK) return done(s);
+        k_lm_compare<U><<<c->sm_count * 4, 256, 0, c->stream>>>(d, check, n, B.mismatches);
+        ++c->launches;
+        TS_CUDA(c, cudaGetLastError());
+        cudaEventRecord(ev.e[0], c->stream);
+        unsigned long long mism = 0;
+        TS_CUDA(c, cudaMemcpyAsync(&mism, B.mismatches, 8, cudaMemcpyDeviceToHost, c->stream));
+        s = finish(c);
+        S.verified = 1;
+        S.verify_mismatches = mism;
+        S.ms_verify = ev.ms(6, 0);
+        if (s == TS_OK && mism)
+            s = fail(c, TS_ERR_INTERNAL, "learned partition: the output differs from the plain sort's");
+    } else {
+        s = finish(c);
+    }
     S.ms_partition += ev.ms(4, 5);
     S.ms_buckets = ev.ms(5, 6);
     return done(s);
@@ -298,6 +376,10 @@ void ts_learned_defaults(ts_learned_params* p) {
     p->max_cdf_error = 0.01f;
     p->use_model = 1;
     p->corrupt_seed = 0;
+    // measured on a B200 (2^28 keys): the partition costs about as much as six
+    // 8-byte passes, and more than four 4-byte passes
+    p->route_passes = 5;
+    p->verify = 0;
 }
 
 ts_status ts_lm_gradients(ts_ctx* c, const float* d_t, const float* d_y, size_t m, int leaves, const int* d_first,

@@ -250,7 +250,7 @@ template <typename U, int XF, int BITS, bool DIVERT = false>
 __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
                                                const unsigned long long* __restrict__ ghist,
                                                unsigned long long* __restrict__ bins, Plan* __restrict__ plan,
-                                               int stable) {
+                                               int stable, unsigned long long* __restrict__ maxb_out) {
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
     __shared__ int live_s[ND];
@@ -288,6 +288,9 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
         if (lane == 0) max_s[warp] = mx;
     }
     __syncthreads();
+    // each digit's largest bucket (0: not live), for callers that estimate
+    // what a sort of more keys from the same distribution would do
+    if (threadIdx.x < ND) maxb_out[threadIdx.x] = live_s[threadIdx.x] ? max_s[threadIdx.x] : 0ull;
     if (threadIdx.x == 0) {
         const unsigned f = st->flags;
         int mode = MODE_SORT;
