@@ -183,6 +183,24 @@ TS_DECLARE_SEGMENTS(f64, double)
  * ts_segments_methods reads (set = 0) or sets (set = 1) the four methods. */
 ts_status ts_segments_autotune(ts_ctx *ctx, size_t key_bytes);
 ts_status ts_segments_methods(ts_ctx *ctx, size_t key_bytes, int *methods, int set);
+/* The plain LSD's autotuner (no counterpart in the crate, whose digit widths
+ * and thresholds are compile-time constants measured on its author's CPUs,
+ * src/radix/mod.rs:38-54). Each onesweep tile variant (keys a thread: 22, 11,
+ * 5 for 4-byte keys; 11, 5, 2 for 8-byte; 32, 16, 8 for 2-byte; 8-bit digits)
+ * is timed on random keys of one length per length bin (n < 2^22, n < 2^25,
+ * larger) and the fastest is kept per key width and bin; ms, if not null,
+ * receives the 3 x 3 median times (bin-major). ts_lsd_variants reads (set = 0)
+ * or sets (set = 1) the three variants of a key width; ts_lsd_variant_ipt
+ * gives a variant's keys a thread. */
+ts_status ts_lsd_autotune(ts_ctx *ctx, size_t key_bytes, float *ms);
+ts_status ts_lsd_variants(ts_ctx *ctx, size_t key_bytes, int *variants, int set);
+int ts_lsd_variant_ipt(size_t key_bytes, int variant);
+/* The tuning cache: the LSD variants and the segmented sort's methods of every
+ * key width, in a JSON file keyed by the GPU's name. _load leaves the context
+ * as it is when the file is missing or was written on another GPU, and sets
+ * *loaded to 1 when it took the file's choices. */
+ts_status ts_ctx_tune_save(ts_ctx *ctx, const char *path);
+ts_status ts_ctx_tune_load(ts_ctx *ctx, const char *path, int *loaded);
 /* Capture and replay CUDA graphs for repeated segmented sorts (on by default). */
 ts_status ts_ctx_use_graphs(ts_ctx *ctx, int on);
 

@@ -29,7 +29,7 @@ __all__ = [
     "Context", "SortByKeyBuffer", "TurbosortError", "apply_order", "default_context", "lib", "sort",
     "sort_by_key", "sort_by_key_with_buffer", "sort_parallel", "sort_segments", "sort_with_buffer", "segments_autotune",
     "segments_methods", "TYPES", "LearnedParams", "LearnedStats", "learned_params", "lm_gradients", "sort_learned",
-    "SortInfo", "divert_skippable_digits",
+    "SortInfo", "divert_skippable_digits", "lsd_variant_ipt",
 ]
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -88,6 +88,11 @@ class SortInfo(ctypes.Structure):
     def as_dict(self) -> dict:
         return {"tier": self.tier, "mode": self.mode, "passes": self.passes, "divert_shift": self.divert_shift,
                 "pass_digit": list(self.pass_digit[:self.passes])}
+
+
+def lsd_variant_ipt(key_bytes: int, variant: int) -> int:
+    """Keys a thread of a plain-LSD tile variant."""
+    return int(lib().ts_lsd_variant_ipt(key_bytes, variant))
 
 
 def divert_skippable_digits(n_live: int, length: int, max_buckets) -> int:
@@ -170,6 +175,16 @@ def lib() -> ctypes.CDLL:
             L.ts_ctx_launches.restype = ctypes.c_ulonglong
             L.ts_ctx_last_sort_info.argtypes = [vp, ctypes.POINTER(SortInfo)]
             L.ts_ctx_last_sort_info.restype = st
+            L.ts_lsd_autotune.argtypes = [vp, sz, ctypes.POINTER(ctypes.c_float)]
+            L.ts_lsd_autotune.restype = st
+            L.ts_lsd_variants.argtypes = [vp, sz, ctypes.POINTER(ctypes.c_int), i]
+            L.ts_lsd_variants.restype = st
+            L.ts_lsd_variant_ipt.argtypes = [sz, i]
+            L.ts_lsd_variant_ipt.restype = i
+            L.ts_ctx_tune_save.argtypes = [vp, ctypes.c_char_p]
+            L.ts_ctx_tune_save.restype = st
+            L.ts_ctx_tune_load.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+            L.ts_ctx_tune_load.restype = st
             L.ts_ctx_test_stall_lookback.argtypes = [vp, ctypes.c_uint32]
             L.ts_ctx_test_stall_lookback.restype = st
             L.ts_divert_skippable_digits.argtypes = [i, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
@@ -240,6 +255,30 @@ class Context:
         """Host-slice sorts of at least min_bytes cross PCIe as `chunks` pieces,
         sorted and merged on the device while the copies run (1 turns it off)."""
         self._check(lib().ts_ctx_transfer_pipeline(self._h, chunks, min_bytes))
+
+    def lsd_autotune(self, key_bytes: int) -> dict:
+        """Time every onesweep tile variant per length bin for keys of this
+        width and keep the fastest; returns the choices and the times."""
+        ms = (ctypes.c_float * 9)()
+        self._check(lib().ts_lsd_autotune(self._h, key_bytes, ms))
+        v = self.lsd_variants(key_bytes)
+        return {"variants": v, "keys_per_thread": [lsd_variant_ipt(key_bytes, x) for x in v],
+                "ms": [[round(ms[b * 3 + x], 4) for x in range(3)] for b in range(3)],
+                "bins": ["n < 2^22", "n < 2^25", "larger"]}
+
+    def lsd_variants(self, key_bytes: int, variants=None) -> list[int]:
+        """The tile variant per length bin for this key width (set when given)."""
+        arr = (ctypes.c_int * 3)(*(variants or [0, 0, 0]))
+        self._check(lib().ts_lsd_variants(self._h, key_bytes, arr, int(variants is not None)))
+        return list(arr)
+
+    def tune_save(self, path: str) -> None:
+        self._check(lib().ts_ctx_tune_save(self._h, os.fsencode(path)))
+
+    def tune_load(self, path: str) -> bool:
+        loaded = ctypes.c_int(0)
+        self._check(lib().ts_ctx_tune_load(self._h, os.fsencode(path), ctypes.byref(loaded)))
+        return bool(loaded.value)
 
     def last_sort_info(self) -> dict:
         """Tier, mode, scatter passes and divert shift of the last plain sort."""

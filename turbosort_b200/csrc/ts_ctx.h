@@ -44,6 +44,10 @@ struct ts_ctx {
     ts::DevBuf pipe_pos[2];        // host-slice pipeline of sort_by_key: position runs
     uint32_t* d_error = nullptr;   // kernel-reported errors, read and cleared by the host
 
+    // plain LSD: the tile variant (k_onesweep keys a thread, halved per step)
+    // per key width (1, 2, 4, 8 bytes) and length bin (< 2^22, < 2^25, more),
+    // set by ts_lsd_autotune; the defaults were measured on a B200
+    int lsd_variant[4][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}};
     // segmented sort: the method of each on-chip length bin per key width
     // (1, 2, 4, 8 bytes), set by the autotuner; and the last captured graph
     int seg_methods[4][4] = {{0, 2, 2, 2}, {0, 2, 2, 2}, {0, 2, 2, 2}, {0, 2, 2, 2}};

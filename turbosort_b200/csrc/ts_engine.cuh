@@ -23,8 +23,15 @@
 namespace ts {
 
 // Tile shapes per key width; 8-bit digits. A tile is 16 warps x 32 lanes x
-// IPT keys.
-template <typename U, bool PAIRS>
+// IPT keys. Variant V halves the keys a thread V times: smaller tiles give a
+// short sort more CTAs to run on (2^20 u32 keys fill only 93 of the largest
+// tiles), larger ones cost less per key on long sorts; the autotuner
+// (ts_lsd_autotune) picks a variant per key width and length bin.
+constexpr int LSD_VARIANTS = 3;
+constexpr int LSD_BINS = 3;  // n < 2^22, n < 2^25, larger
+static inline int lsd_bin(size_t n) { return n < ((size_t)1 << 22) ? 0 : n < ((size_t)1 << 25) ? 1 : 2; }
+
+template <typename U, bool PAIRS, int V = 0>
 struct LsdCfg {
     static constexpr int BITS = 8;
     static constexpr int THREADS = 512;
@@ -40,7 +47,9 @@ struct LsdCfg {
     // the per-tile costs (look-back, counter scans) shrink per key as tiles
     // grow, which on a B200 outweighs double-buffering a smaller tile
     // (2^28 u32 keys: 15 keys a thread double-buffered 5.18 ms, 22 single 4.83 ms)
-    static constexpr int IPT = sizeof(U) == 8 ? (PAIRS ? 7 : 11) : (PAIRS ? 11 : (sizeof(U) == 4 ? 22 : 32));
+    static constexpr int IPT0 = sizeof(U) == 8 ? (PAIRS ? 7 : 11) : (PAIRS ? 11 : (sizeof(U) == 4 ? 22 : 32));
+    static constexpr int IPT = IPT0 >> V;
+    static_assert(V >= 0 && V < LSD_VARIANTS && IPT >= 1, "tile variant");
     static constexpr int NBUF = 1;  // tiles of keys in flight per CTA; the next one is prefetched into L2
     // items with i % MATCH_MOD < MATCH_CNT find their digit's peers with
     // match.any, the rest with ballots: a share of the items keeps the match
@@ -96,6 +105,8 @@ static int occupancy(ts_ctx*, K kernel, int threads, size_t smem) {
 }
 
 static inline bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+// row of the per-width tuning tables: 1, 2, 4, 8 bytes
+static inline int width_slot(size_t bytes) { return bytes == 1 ? 0 : bytes == 2 ? 1 : bytes == 4 ? 2 : 3; }
 
 // The LSD passes over `in` (n keys), writing through pp[0]/pp[1]; with PAIRS
 // the positions ping-pong through vpp and the last pass writes `vout`.
@@ -242,11 +253,19 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
             if ((s = grow(c, c->runs, runs_cap * 8, "divert runs")) != TS_OK) return s;
             occupancy_of((const void*)k_divert_long<U, XF>, SEG_THREADS, MSD_SMEM);
         }
+        const int variant = c->lsd_variant[width_slot(sizeof(U))][lsd_bin(n)];
         auto enqueue = [&]() -> ts_status {
             Plan* plan = nullptr;
             ts_status st;
-            if ((st = run_lsd<U, XF, false>(c, d_data, d_alt, d_data, nullptr, nullptr, nullptr, n, 1, &plan)) != TS_OK)
-                return st;
+            if (variant == 1)
+                st = run_lsd<U, XF, false, LsdCfg<U, false, 1>>(c, d_data, d_alt, d_data, nullptr, nullptr, nullptr, n,
+                                                                1, &plan);
+            else if (variant == 2)
+                st = run_lsd<U, XF, false, LsdCfg<U, false, 2>>(c, d_data, d_alt, d_data, nullptr, nullptr, nullptr, n,
+                                                                1, &plan);
+            else
+                st = run_lsd<U, XF, false>(c, d_data, d_alt, d_data, nullptr, nullptr, nullptr, n, 1, &plan);
+            if (st != TS_OK) return st;
             mark(c, "finish");
             const int grid = c->sm_count * 4;
             k_finish_keys<U><<<grid, 512, 0, c->stream>>>(plan, d_alt, d_data, n, aligned16(d_alt) && aligned16(d_data));
@@ -274,8 +293,9 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         if (c->stream) cudaStreamIsCapturing(c->stream, &cs);
         if (!c->use_graphs || !c->stream || c->timing || c->test_spin_limit || cs != cudaStreamCaptureStatusNone)
             return enqueue();
-        const size_t key[9] = {sizeof(U) * 4 + (size_t)XF, (size_t)d_data, (size_t)d_alt, n, (size_t)c->meta.p,
-                               (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p, (size_t)c->runs.p};
+        const size_t key[9] = {sizeof(U) * 64 + (size_t)XF * 8 + (size_t)variant, (size_t)d_data, (size_t)d_alt, n,
+                               (size_t)c->meta.p, (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p,
+                               (size_t)c->runs.p};
         if (c->sort_graph && std::memcmp(key, c->sort_graph_key, sizeof key) == 0) {
             TS_CUDA(c, cudaGraphLaunch(c->sort_graph, c->stream));
             c->launches += c->sort_graph_launches;

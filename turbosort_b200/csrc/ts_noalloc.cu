@@ -71,6 +71,9 @@ ts_status setup(int device, ts_ctx** out) {
     }
     c->own_stream = false;
     c->use_graphs = false;  // instantiating a graph could allocate
+    // the scratch is sized for the largest tiles (fewest look-back entries)
+    for (auto& row : c->lsd_variant)
+        for (int& v : row) v = 0;
     c->alt.p = base;
     c->alt.cap = kAltBytes;
     c->lookback.p = base + kAltBytes;
