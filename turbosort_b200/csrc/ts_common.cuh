@@ -64,11 +64,11 @@ constexpr int LB_WINDOW = 4;                 // look-back entries loaded per rou
 constexpr uint32_t ERR_TIMEOUT = 1u;
 constexpr uint32_t ERR_BOUNDS = 2u;
 
-// What the upfront scan found (written by k_scan, read by k_hist / k_plan).
+// What the upfront scan found (written by k_scan, read by k_hist).
 struct ScanState {
     unsigned long long diff;    // OR of (key ^ first key): the bits that vary
     unsigned int flags;         // bit 0: some pair descends; bit 1: some pair ascends
-    unsigned int pad;
+    unsigned int hist_done;     // k_hist CTAs that have added their counts
 };
 constexpr unsigned SCAN_NOT_ASC = 1u;
 constexpr unsigned SCAN_NOT_DESC = 2u;

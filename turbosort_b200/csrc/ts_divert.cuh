@@ -1,7 +1,7 @@
 // ts_divert.cuh — finishing the runs a diverted sort leaves
 // (src/radix/divert.rs:60-81).
 //
-// When k_plan diverts, the passes sort only the digits from divert_shift up:
+// When the plan diverts, the passes sort only the digits from divert_shift up:
 // the keys then come out ordered by that prefix, in runs of keys sharing it
 // (most runs one key long), and each run only needs sorting within itself.
 //   k_divert_runs  one read of the keys, 16-byte loads, 32 * KPT consecutive

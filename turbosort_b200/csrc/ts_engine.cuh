@@ -38,7 +38,7 @@ struct LsdCfg {
     // the first live pass of a keys-only sort ranks with shared atomics
     // (k_onesweep, UNSTABLE1)
     static constexpr bool UNSTABLE1 = true;
-    // 8-byte keys without positions divert (src/radix/divert.rs): k_plan may
+    // 8-byte keys without positions divert (src/radix/divert.rs): the plan may
     // leave out the lowest live digits, and k_divert_runs / k_divert_long
     // finish the runs that leaves
     static constexpr bool DIVERT = !PAIRS && sizeof(U) == 8;
@@ -91,7 +91,8 @@ struct MetaLayout {
     // in the (zeroed) plan area, after the Plan: the diverted sort's count of
     // listed runs (u64) and its work counter (u32)
     size_t divert_off() const { return plan_off + 128; }
-    // after those: the largest bucket of each digit (u64, 0 when not live)
+    // after those: the largest bucket of each digit (u64, 0 when not live),
+    // which the plan writes
     size_t maxb_off() const { return plan_off + 144; }
 };
 static_assert(sizeof(Plan) <= 128, "the plan area holds the Plan and the divert counters");
@@ -146,16 +147,13 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     {
         constexpr int T = 1024;
         const size_t smem = (size_t)ND * RADIX * hist_copies<RADIX, ND>() * 4;
-        auto kern = k_hist<U, XF, C::BITS, T>;
+        static_assert(144 + 8 * ND <= 256, "the plan area holds every digit's largest bucket");
+        auto kern = k_hist<U, XF, C::BITS, T, C::DIVERT>;
         const int occ = occupancy(c, kern, T, smem);
-        kern<<<c->sm_count * occ, T, smem, c->stream>>>(in, n, st, hist, vec_ok);
+        kern<<<c->sm_count * occ, T, smem, c->stream>>>(in, n, st, hist, vec_ok, bins, plan, PAIRS ? 1 : 0,
+                                                         (unsigned long long*)(meta + m.maxb_off()));
         ++c->launches;
     }
-    mark(c, "plan");
-    static_assert(144 + 8 * ND <= 256, "the plan area holds every digit's largest bucket");
-    k_plan<U, XF, C::BITS, C::DIVERT><<<1, 1024, 0, c->stream>>>(in, n, st, hist, bins, plan, PAIRS ? 1 : 0,
-                                                                 (unsigned long long*)(meta + m.maxb_off()));
-    ++c->launches;
     {
         using Sm = typename C::Smem;
         auto kern = n <= (size_t)0x7fffffff

@@ -5,7 +5,8 @@
 //               (src/presorted.rs:15-65)
 //   k_hist      one read: histograms of every varying digit
 //               (src/radix/histogram.rs:15-110)
-//   k_plan      live passes (src/radix/mod.rs:229-239) and the exclusive scans
+//               and, in its last CTA to finish, the plan: live passes
+//               (src/radix/mod.rs:229-239), diverting, and the exclusive scans
 //               (src/radix/prefix_sum.rs:17-24), decided on the device
 //   k_onesweep  one stable scatter pass per live digit
 //               (src/radix/scatter.rs:26-247): warp ranking with match.any,
@@ -151,9 +152,17 @@ __host__ __device__ constexpr int hist_copies() {
     return RADIX <= 256 ? (ND <= 4 ? 32 : 16) : 1;
 }
 
-template <typename U, int XF, int BITS, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
-                                                  unsigned long long* __restrict__ ghist, int vec_ok) {
+template <typename U, int XF, int BITS, bool DIVERT>
+__device__ void plan_body(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
+                          const unsigned long long* ghist, unsigned long long* __restrict__ bins,
+                          Plan* __restrict__ plan, int stable, unsigned long long* __restrict__ maxb_out);
+
+template <typename U, int XF, int BITS, int THREADS, bool DIVERT>
+__global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, size_t n, ScanState* __restrict__ st,
+                                                  unsigned long long* __restrict__ ghist, int vec_ok,
+                                                  unsigned long long* __restrict__ bins, Plan* __restrict__ plan,
+                                                  int stable, unsigned long long* __restrict__ maxb_out) {
+    static_assert(THREADS >= 32 * ((Bits<U>::W + BITS - 1) / BITS), "the plan scans a digit a warp");
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
     constexpr int COPIES = hist_copies<RADIX, ND>();
@@ -206,6 +215,16 @@ __global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, siz
         for (int c = 0; c < COPIES; ++c) s += h_s[i * COPIES + ((c + i) & (COPIES - 1))];
         if (s) atomicAdd(&ghist[i], (unsigned long long)s);
     }
+    // the last CTA to finish makes the plan (one launch fewer than a
+    // separate plan kernel): its ticket comes after every other CTA's counts
+    __shared__ int last_s;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last_s = atomicAdd(&st->hist_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last_s) return;
+    __threadfence();
+    plan_body<U, XF, BITS, DIVERT>(src, n, st, ghist, bins, plan, stable, maxb_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -238,7 +257,8 @@ __host__ __device__ inline int skippable_digits(int n_live, unsigned long long l
 }
 
 // ---------------------------------------------------------------------------
-// k_plan: one CTA. Live passes are the counted digits whose histogram does
+// The plan, by one CTA of at least 32 * ND threads (k_hist's last). Live
+// passes are the counted digits whose histogram does
 // not hold every key in the first key's bucket; each gets its exclusive scan.
 // `stable` (sort_by_key) leaves descending input to the passes, since a
 // plain reversal would reverse equal keys. With DIVERT (keys only) the
@@ -246,11 +266,10 @@ __host__ __device__ inline int skippable_digits(int n_live, unsigned long long l
 // (src/radix/mod.rs:240-242), and divert_shift tells the finishing kernels
 // which runs remain.
 // ---------------------------------------------------------------------------
-template <typename U, int XF, int BITS, bool DIVERT = false>
-__global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
-                                               const unsigned long long* __restrict__ ghist,
-                                               unsigned long long* __restrict__ bins, Plan* __restrict__ plan,
-                                               int stable, unsigned long long* __restrict__ maxb_out) {
+template <typename U, int XF, int BITS, bool DIVERT>
+__device__ void plan_body(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
+                          const unsigned long long* ghist, unsigned long long* __restrict__ bins,
+                          Plan* __restrict__ plan, int stable, unsigned long long* __restrict__ maxb_out) {
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
     __shared__ int live_s[ND];
@@ -260,7 +279,7 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
     if (threadIdx.x < ND) {
         const int d = threadIdx.x;
         const bool counted = ((diff >> (d * BITS)) & (unsigned long long)(RADIX - 1)) != 0;
-        live_s[d] = counted && ghist[(size_t)d * RADIX + digit_of(first, d * BITS, RADIX - 1)] < n;
+        live_s[d] = counted && __ldcg(&ghist[(size_t)d * RADIX + digit_of(first, d * BITS, RADIX - 1)]) < n;
     }
     __syncthreads();
     // warp w scans digit w's histogram
@@ -269,7 +288,7 @@ __global__ void __launch_bounds__(1024) k_plan(const U* __restrict__ src, size_t
         unsigned long long carry = 0, mx = 0;
         for (int r0 = 0; r0 < RADIX; r0 += 32) {
             const int r = r0 + lane;
-            unsigned long long v = r < RADIX ? ghist[(size_t)warp * RADIX + r] : 0ull;
+            unsigned long long v = r < RADIX ? __ldcg(&ghist[(size_t)warp * RADIX + r]) : 0ull;
             mx = v > mx ? v : mx;
             unsigned long long x = v;
 #pragma unroll
