@@ -169,20 +169,39 @@ def ncu_traffic(name: str):
     return None
 
 
-def cpu_sample_rate(kind: str, dist: int, n_full: int, budget_s: float, threads: int, seed: int):
-    """The oracle's sort_parallel (the crate's algorithm restated in C) on a
-    bounded sample of the workload: returns (GKeys/s, sample description)."""
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_sample_rate(kind: str, dist: int, n_full: int, budget_s: float, threads: int, seed: int,
+                    serial: bool = False):
+    """The oracle's sort_parallel, or with `serial` its sort on one core (the
+    crate's algorithm restated in C), on a bounded sample of the workload:
+    returns (GKeys/s, sample description)."""
     from oracle import oracle as O
 
     n = min(n_full, 1 << 24)
     base = gen(kind, dist, n, seed)
     work = base.copy()
-    O.sort_parallel_inplace(work, threads)  # warm-up
+
+    def run(a):
+        if serial:
+            O.sort_inplace(a)
+        else:
+            O.sort_parallel_inplace(a, threads)
+
+    run(work)  # warm-up
     reps, total = 0, 0.0
     while total < budget_s and reps < 50:
         np.copyto(work, base)
         t0 = time.perf_counter()
-        O.sort_parallel_inplace(work, threads)
+        run(work)
         total += time.perf_counter() - t0
         reps += 1
     return n * reps / total / 1e9, f"{reps} sorts of 2^{n.bit_length() - 1} keys of the same distribution"
@@ -501,7 +520,9 @@ def bench_learned(ts, torch, ctx, kind, steps, warmup, peak, lg=28, buckets_log2
     tdt = {"lognormal_f64": torch.float64, "gauss_mix_u64": torch.uint64, "unit_f32_dups": torch.float32}[kind]
     master = torch.from_numpy(host.view(np.int64 if w == 8 else np.int32)).to(dev)
     d = torch.empty_like(master)
-    p = ts.learned_params(buckets_log2=buckets_log2)
+    # the partition itself (the cost route off), against the plain sort with
+    # and without diverting
+    p = ts.learned_params(buckets_log2=buckets_log2, route_passes=0)
 
     def timed(fn):
         tot = 0.0
@@ -519,9 +540,17 @@ def bench_learned(ts, torch, ctx, kind, steps, warmup, peak, lg=28, buckets_log2
         return tot / steps, r
 
     ms_plain, _ = timed(lambda: ts.sort(d.view(tdt), ctx))
+    plain_info = ctx.last_sort_info()
     plain_out = d.clone()
+    ctx.set_divert(False)
+    ms_plain_all, _ = timed(lambda: ts.sort(d.view(tdt), ctx))
+    all_info = ctx.last_sort_info()
+    ctx.set_divert(True)
+    ok_all = bool(torch.equal(d, plain_out))
+    d.copy_(master)
+    st_default = ts.sort_learned(d.view(tdt), ts.learned_params(buckets_log2=buckets_log2), ctx)
     ms_learned, st = timed(lambda: ts.sort_learned(d.view(tdt), p, ctx))
-    ok = bool(torch.equal(d, plain_out))
+    ok = bool(torch.equal(d, plain_out)) and ok_all
     # both byte-equal to numpy's sort of the input's radix keys
     ok &= check_exact(plain_out.cpu().numpy().view(host.dtype), expected_radix(host))
     del host
@@ -535,13 +564,19 @@ def bench_learned(ts, torch, ctx, kind, steps, warmup, peak, lg=28, buckets_log2
     return {"gkeys_s": round(n / (ms_learned / 1e3) / 1e9, 3), "ms": round(ms_learned, 3),
             "plain_gkeys_s": round(n / (ms_plain / 1e3) / 1e9, 3), "plain_ms": round(ms_plain, 3),
             "speedup_vs_plain": round(ms_plain / ms_learned, 3),
+            "plain_passes": plain_info["passes"], "plain_divert_shift": plain_info["divert_shift"],
+            "plain_all_passes_ms": round(ms_plain_all, 3), "plain_all_passes": all_info["passes"],
+            "speedup_vs_plain_all_passes": round(ms_plain_all / ms_learned, 3),
+            "default_route": {"routed_to_plain": int(st_default["reason"] == 4),
+                              "est_plain_passes": st_default["est_plain_passes"]},
             "roofline_frac": round(learned_bytes / (ms_learned / 1e3) / 1e9 / peak, 3),
             "fell_back": st["fell_back"], "reason": st["reason"], "imbalance": round(st["imbalance"], 3),
             "max_bucket": st["max_bucket"], "max_cdf_error": round(st["max_cdf_error"], 5),
             "train_loss": [st["train_loss_first"], st["train_loss_last"]],
             "phase_ms": {k2: round(st[k2], 3) for k2 in ("ms_sample", "ms_train", "ms_partition", "ms_buckets")},
             "launches": int(launches), "keys": n, "ok": ok,
-            "checks": "learned output == plain device sort output == numpy's sort of the radix keys (bytes)"}
+            "checks": "learned output == plain device sort output (with and without diverting) == numpy's sort "
+                      "of the radix keys (bytes)"}
 
 
 def main() -> None:
@@ -648,20 +683,20 @@ def main() -> None:
         pinned = torch.empty(n * w, dtype=torch.uint8, pin_memory=True).numpy().view(NP[kind])
         want = expected_radix(host)
 
-        def host_calls(steps):
+        def host_calls(steps, buf):
             e_ms, ok = [], True
             for i in range(args.warmup + steps):
-                np.copyto(pinned, host)
+                np.copyto(buf, host)
                 torch.cuda.synchronize()
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record()
-                ts.sort(pinned, ctx)
+                ts.sort(buf, ctx)
                 e1.record()
                 torch.cuda.synchronize()
                 if i >= args.warmup:
                     e_ms.append(e0.elapsed_time(e1))
-            ok = check_exact(pinned, want)
+            ok = check_exact(buf, want)
             total = sum(e_ms)
             if dist_mod is not None:
                 t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
@@ -670,26 +705,38 @@ def main() -> None:
             return total, ok
 
         ctx.transfer_pipeline(PIPE_CHUNKS, PIPE_MIN_BYTES)
-        emax, ok = host_calls(args.steps)
+        emax, ok = host_calls(args.steps, pinned)
         serial_steps = max(1, min(args.steps, 5))
         ctx.transfer_pipeline(1, PIPE_MIN_BYTES)
-        smax, sok = host_calls(serial_steps)
+        smax, sok = host_calls(serial_steps, pinned)
         ctx.transfer_pipeline(PIPE_CHUNKS, PIPE_MIN_BYTES)
+        # the same call on pageable host memory (what a Rust &mut [T] usually is)
+        del pinned
+        pageable = np.empty(n, dtype=NP[kind])
+        pmax, pok = host_calls(serial_steps, pageable)
+        del pageable
         line["e2e"] = {"value": round(world * n * args.steps / (emax / 1e3) / 1e9, 3), "unit": "GKeys/s",
                        "h2d_bytes_per_step": n * w, "d2h_bytes_per_step": n * w,
                        "ms_per_step": round(emax / args.steps, 3),
                        "call": f"ts_sort_{kind} on pinned host memory",
                        "pipeline": {"chunks": PIPE_CHUNKS, "min_bytes": PIPE_MIN_BYTES,
                                     "serial_ms_per_step": round(smax / serial_steps, 3)},
-                       "bit_exact_checks": "byte-equal to numpy's sort" if ok and sok else "FAILED"}
-        del pinned
+                       "pageable": {"value": round(world * n * serial_steps / (pmax / 1e3) / 1e9, 3),
+                                    "ms_per_step": round(pmax / serial_steps, 3),
+                                    "call": f"ts_sort_{kind} on pageable host memory (pinned staging slots)"},
+                       "bit_exact_checks": "byte-equal to numpy's sort" if ok and sok and pok else "FAILED"}
 
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         rate, sample = cpu_sample_rate(kind, dist, n, 15.0, threads, 0x9E3779B97F4A7C15)
         line["cpu_baseline"] = {"value": round(rate, 4), "unit": "GKeys/s", "cores": threads, "kind": "port",
-                                "sample": sample,
+                                "sample": sample, "cpu": cpu_model(),
                                 "what": "turbosort sort_parallel (src/parallel.rs) restated in C, pthreads"}
+        rate1, sample1 = cpu_sample_rate(kind, dist, n, 10.0, 1, 0x9E3779B97F4A7C15, serial=True)
+        line["cpu_baseline_serial"] = {"value": round(rate1, 4), "unit": "GKeys/s", "cores": 1, "kind": "port",
+                                       "sample": sample1, "cpu": cpu_model(),
+                                       "what": "turbosort sort (src/lib.rs:99, src/dispatch.rs:31) restated in C, "
+                                               "one core"}
 
     if not args.no_breakdown:
         bd = {}

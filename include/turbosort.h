@@ -100,6 +100,11 @@ typedef struct ts_sort_info {
 } ts_sort_info;
 ts_status ts_ctx_last_sort_info(ts_ctx *ctx, ts_sort_info *info);
 
+/* Diverting of 8-byte keys (on by default, as the crate's sort always
+ * diverts when its rule allows, src/radix/mod.rs:240-242). Off, every live
+ * digit gets a pass; the output is the same. For comparisons. */
+ts_status ts_ctx_set_divert(ts_ctx *ctx, int on);
+
 /* Test hook for failure detection, no counterpart in the crate: in the next
  * LSD sort on this context (keys or order, more than 4096 keys), the first
  * scatter pass's tile 0 never publishes its look-back entry, and every wait

@@ -169,17 +169,27 @@ def test_ablation_on_float_keys(ts, W, kind):
 
 
 def test_training_improves_the_fit(ts, W):
-    """What the training does: from heights that interpolate the sample's CDF
-    at the breakpoints, the Adam steps lower the squared rank error over all
-    the leaf's samples, without costing balance."""
+    """What the training gains over the same model untrained (train_iters =
+    0, heights that interpolate the sample's CDF at the breakpoints): the Adam
+    steps lower the squared rank error over all of each leaf's samples on both
+    skewed inputs (by a third or more), and on the Gaussian mixture, whose
+    modes the untrained leaves straddle, they shrink the largest bucket
+    (measured 2834 -> 2589 keys at 2^24, 45263 -> 39034 at 2^28). On the
+    lognormal input the untrained model's buckets are already as even, and on
+    neither does the bucket finish get faster: the gain is the fit and the
+    worst bucket, not time."""
     for kind in ("gauss_mix_u64", "lognormal_f64"):
         a = inputs(W, kind, n=1 << 24)
         st0 = ts.sort_learned(a.copy(), train_iters=0, overflow_factor=1e9)
-        st1 = ts.sort_learned(a.copy())
+        st1 = ts.sort_learned(a.copy(), overflow_factor=1e9)
+        assert st1["train_iters"] > 0
         assert st0["train_loss_first"] == pytest.approx(st0["train_loss_last"], rel=1e-9)
         assert st1["train_loss_first"] == pytest.approx(st0["train_loss_last"], rel=1e-4)
-        assert st1["train_loss_last"] < 0.9 * st1["train_loss_first"]
-        assert st1["imbalance"] <= 1.25 * st0["imbalance"]
+        assert st1["train_loss_last"] < 0.75 * st1["train_loss_first"]
+        if kind == "gauss_mix_u64":
+            assert st1["max_bucket"] < 0.95 * st0["max_bucket"], (st0["max_bucket"], st1["max_bucket"])
+        else:
+            assert st1["max_bucket"] <= 1.05 * st0["max_bucket"], (st0["max_bucket"], st1["max_bucket"])
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
@@ -288,19 +298,23 @@ def test_full_size_equals_plain_sort(ts, W):
     assert torch.equal(a.view(torch.int64), b.view(torch.int64))
 
 
-@pytest.mark.parametrize("kind, routed", [("unit_f32_dups", True), ("uniform_u32", True), ("uniform_u64", True),
-                                          ("lognormal_f64", False), ("gauss_mix_u64", False)])
-def test_cost_route(ts, W, kind, routed):
+@pytest.mark.parametrize("kind, n, routed", [("unit_f32_dups", N, True), ("uniform_u32", N, True),
+                                             ("uniform_u64", N, True), ("lognormal_f64", N, True),
+                                             ("gauss_mix_u64", 1 << 26, False)])
+def test_cost_route(ts, W, kind, n, routed):
     """With the default route, inputs the plain sort handles in at most five
-    passes (every 4-byte key; random 8-byte keys, which it diverts to four)
-    take the plain sort; skewed 8-byte keys that need all eight passes take
-    the partition. The output is the oracle's either way."""
+    passes take the plain sort: every 4-byte key, random 8-byte keys (which
+    it diverts to four passes), and at 2^21 the lognormal f64 keys, whose top
+    digits already carry the 23 bits that diverting needs there. At 2^26 the
+    Gaussian mixture's top digits split the keys too poorly to divert, all
+    eight passes would run, and the partition takes it. The output is the
+    oracle's either way."""
     import turbosort_b200 as real
 
-    a = inputs(W, kind)
+    a = inputs(W, kind, n=n)
     got = a.copy()
     st = real.sort_learned(got)
-    same_bits(got, O.sort(a))
+    same_bits(got, O.sort_parallel(a))
     if routed:
         assert st["fell_back"] == 1 and st["reason"] == 4, st
         assert 0 < st["est_plain_passes"] <= 5, st

@@ -185,6 +185,8 @@ def lib() -> ctypes.CDLL:
             L.ts_ctx_tune_save.restype = st
             L.ts_ctx_tune_load.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
             L.ts_ctx_tune_load.restype = st
+            L.ts_ctx_set_divert.argtypes = [vp, i]
+            L.ts_ctx_set_divert.restype = st
             L.ts_ctx_test_stall_lookback.argtypes = [vp, ctypes.c_uint32]
             L.ts_ctx_test_stall_lookback.restype = st
             L.ts_divert_skippable_digits.argtypes = [i, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
@@ -279,6 +281,10 @@ class Context:
         loaded = ctypes.c_int(0)
         self._check(lib().ts_ctx_tune_load(self._h, os.fsencode(path), ctypes.byref(loaded)))
         return bool(loaded.value)
+
+    def set_divert(self, on: bool) -> None:
+        """Diverting of 8-byte keys (on by default); off, every live digit gets a pass."""
+        self._check(lib().ts_ctx_set_divert(self._h, int(on)))
 
     def last_sort_info(self) -> dict:
         """Tier, mode, scatter passes and divert shift of the last plain sort."""

@@ -424,6 +424,12 @@ ts_status ts_ctx_last_sort_info(ts_ctx* c, ts_sort_info* info) {
     return TS_OK;
 }
 
+ts_status ts_ctx_set_divert(ts_ctx* c, int on) {
+    if (!c) return TS_ERR_INVALID;
+    c->divert = on != 0;
+    return TS_OK;
+}
+
 ts_status ts_ctx_test_stall_lookback(ts_ctx* c, uint32_t spin_limit) {
     if (!c) return TS_ERR_INVALID;
     c->test_spin_limit = spin_limit;

@@ -75,6 +75,8 @@ struct ts_ctx {
     std::vector<cudaEvent_t> stage_events; // the last DMA of each slot
     ts::CopyPool* copy_pool = nullptr;
 
+    // diverting of 8-byte keys (ts_ctx_set_divert), on by default as in the crate
+    bool divert = true;
     // test hook (ts_ctx_test_stall_lookback): the next LSD sort's first pass
     // withholds tile 0's look-back entry and gives up after this many rounds
     uint32_t test_spin_limit = 0;

@@ -84,10 +84,29 @@ __device__ void divert_sort_short(U* d, size_t s, size_t len) {
         for (size_t j = 0; j < len; ++j) d[s + j] = from_key<U, XF>(k[j]);
 }
 
-// KPT keys a lane, consecutive (16-byte loads when the keys are aligned),
-// a warp 32 * KPT consecutive keys per step, two steps' loads in flight.
+// A run of three or more keys starting at i: its end, then a sort by this
+// thread or a place in the list. Rare, so kept out of the streaming loop.
 template <typename U, int XF>
-__global__ void __launch_bounds__(256) k_divert_runs(const Plan* __restrict__ plan, U* d, size_t n,
+__device__ __noinline__ void divert_long_run(U* d, size_t n, size_t i, int shift, unsigned long long* runs,
+                                             unsigned long long* n_runs, size_t runs_cap, uint32_t* error) {
+    const size_t end = divert_run_end<U, XF>(d, n, i, shift);
+    const size_t len = end - i;
+    if (len <= (size_t)DIVERT_SHORT) {
+        divert_sort_short<U, XF>(d, i, len);
+    } else {
+        const unsigned long long slot = atomicAdd(n_runs, 1ull);
+        if (slot < runs_cap) runs[slot] = i;
+        else atomicOr(error, ERR_BOUNDS);  // cannot happen: a listed run holds more than DIVERT_SHORT keys
+    }
+}
+
+// KPT keys a lane, consecutive (16-byte loads when the keys are aligned), a
+// warp 32 * KPT consecutive keys per step. A key starts a run of two or more
+// when its prefix differs from the key before and equals the key after; the
+// key after that tells whether the run has exactly two keys, which are then
+// ordered from registers (most runs); longer runs take the slow path.
+template <typename U, int XF>
+__global__ void __launch_bounds__(256, 4) k_divert_runs(const Plan* __restrict__ plan, U* d, size_t n,
                                                      unsigned long long* __restrict__ runs,
                                                      unsigned long long* __restrict__ n_runs, size_t runs_cap,
                                                      uint32_t* __restrict__ error, int vec_ok) {
@@ -99,8 +118,9 @@ __global__ void __launch_bounds__(256) k_divert_runs(const Plan* __restrict__ pl
     const int lane = threadIdx.x & 31;
     const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
-    auto load = [&](size_t base, U (&k)[KPT]) {
-        const size_t i0 = base + (size_t)lane * KPT;
+    for (size_t wb = gw * W; wb < n; wb += nw * W) {  // warp-uniform
+        const size_t i0 = wb + (size_t)lane * KPT;
+        U k[KPT + 2];  // this lane's keys, then the next two
         if (vec_ok && i0 + KPT <= n) {
             const uint4* p = reinterpret_cast<const uint4*>(d + i0);
             union {
@@ -115,44 +135,34 @@ __global__ void __launch_bounds__(256) k_divert_runs(const Plan* __restrict__ pl
 #pragma unroll
             for (int e = 0; e < KPT; ++e) k[e] = i0 + e < n ? d[i0 + e] : (U)0;
         }
-    };
-    auto step = [&](size_t base, const U (&k)[KPT]) {
-        const size_t i0 = base + (size_t)lane * KPT;
         U prev = __shfl_up_sync(0xffffffffu, k[KPT - 1], 1);
-        U next = __shfl_down_sync(0xffffffffu, k[0], 1);
+        k[KPT] = __shfl_down_sync(0xffffffffu, k[0], 1);
+        k[KPT + 1] = __shfl_down_sync(0xffffffffu, k[1], 1);
         if (lane == 0 && i0 > 0 && i0 < n) prev = d[i0 - 1];
-        if (lane == 31 && i0 + KPT < n) next = d[i0 + KPT];
+        if (lane == 31) {
+            if (i0 + KPT < n) k[KPT] = d[i0 + KPT];
+            if (i0 + KPT + 1 < n) k[KPT + 1] = d[i0 + KPT + 1];
+        }
         unsigned long long pp = pre(prev);
+        unsigned long long p[KPT + 2];
+#pragma unroll
+        for (int e = 0; e < KPT + 2; ++e) p[e] = pre(k[e]);
 #pragma unroll
         for (int e = 0; e < KPT; ++e) {
             const size_t i = i0 + e;
-            if (i >= n) break;
-            const unsigned long long p = pre(k[e]);
-            const bool start = i == 0 || pp != p;
-            pp = p;
-            if (!start || i + 1 >= n) continue;
-            const unsigned long long pn = pre(e + 1 < KPT ? k[e + 1] : next);
-            if (pn != p) continue;
-            // a run of two or more keys starts here
-            const size_t end = divert_run_end<U, XF>(d, n, i, shift);
-            const size_t len = end - i;
-            if (len <= (size_t)DIVERT_SHORT) {
-                divert_sort_short<U, XF>(d, i, len);
+            const bool start = i == 0 || pp != p[e];
+            pp = p[e];
+            if (i + 1 >= n || !start || p[e + 1] != p[e]) continue;
+            if (i + 2 >= n || p[e + 2] != p[e]) {
+                // exactly two keys
+                if (to_key<U, XF>(k[e]) > to_key<U, XF>(k[e + 1])) {
+                    d[i] = k[e + 1];
+                    d[i + 1] = k[e];
+                }
             } else {
-                const unsigned long long slot = atomicAdd(n_runs, 1ull);
-                if (slot < runs_cap) runs[slot] = i;
-                else atomicOr(error, ERR_BOUNDS);  // cannot happen: a listed run holds more than DIVERT_SHORT keys
+                divert_long_run<U, XF>(d, n, i, shift, runs, n_runs, runs_cap, error);
             }
         }
-    };
-    for (size_t wb = gw * W; wb < n; wb += 2 * nw * W) {  // warp-uniform
-        U a[KPT], b[KPT];
-        load(wb, a);
-        const size_t wb2 = wb + nw * W;
-        const bool two = wb2 < n;  // warp-uniform
-        if (two) load(wb2, b);
-        step(wb, a);
-        if (two) step(wb2, b);
     }
 }
 

@@ -151,7 +151,8 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         auto kern = k_hist<U, XF, C::BITS, T, C::DIVERT>;
         const int occ = occupancy(c, kern, T, smem);
         kern<<<c->sm_count * occ, T, smem, c->stream>>>(in, n, st, hist, vec_ok, bins, plan, PAIRS ? 1 : 0,
-                                                         (unsigned long long*)(meta + m.maxb_off()));
+                                                         (unsigned long long*)(meta + m.maxb_off()),
+                                                         c->divert ? 1 : 0);
         ++c->launches;
     }
     {
@@ -291,7 +292,8 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         if (c->stream) cudaStreamIsCapturing(c->stream, &cs);
         if (!c->use_graphs || !c->stream || c->timing || c->test_spin_limit || cs != cudaStreamCaptureStatusNone)
             return enqueue();
-        const size_t key[9] = {sizeof(U) * 64 + (size_t)XF * 8 + (size_t)variant, (size_t)d_data, (size_t)d_alt, n,
+        const size_t key[9] = {sizeof(U) * 128 + (size_t)XF * 16 + (size_t)variant * 2 + (c->divert ? 1 : 0),
+                               (size_t)d_data, (size_t)d_alt, n,
                                (size_t)c->meta.p, (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p,
                                (size_t)c->runs.p};
         if (c->sort_graph && std::memcmp(key, c->sort_graph_key, sizeof key) == 0) {

@@ -155,13 +155,15 @@ __host__ __device__ constexpr int hist_copies() {
 template <typename U, int XF, int BITS, bool DIVERT>
 __device__ void plan_body(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
                           const unsigned long long* ghist, unsigned long long* __restrict__ bins,
-                          Plan* __restrict__ plan, int stable, unsigned long long* __restrict__ maxb_out);
+                          Plan* __restrict__ plan, int stable, unsigned long long* __restrict__ maxb_out,
+                          int divert);
 
 template <typename U, int XF, int BITS, int THREADS, bool DIVERT>
 __global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, size_t n, ScanState* __restrict__ st,
                                                   unsigned long long* __restrict__ ghist, int vec_ok,
                                                   unsigned long long* __restrict__ bins, Plan* __restrict__ plan,
-                                                  int stable, unsigned long long* __restrict__ maxb_out) {
+                                                  int stable, unsigned long long* __restrict__ maxb_out,
+                                                  int divert) {
     static_assert(THREADS >= 32 * ((Bits<U>::W + BITS - 1) / BITS), "the plan scans a digit a warp");
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, siz
     __syncthreads();
     if (!last_s) return;
     __threadfence();
-    plan_body<U, XF, BITS, DIVERT>(src, n, st, ghist, bins, plan, stable, maxb_out);
+    plan_body<U, XF, BITS, DIVERT>(src, n, st, ghist, bins, plan, stable, maxb_out, divert);
 }
 
 // ---------------------------------------------------------------------------
@@ -269,7 +271,8 @@ __host__ __device__ inline int skippable_digits(int n_live, unsigned long long l
 template <typename U, int XF, int BITS, bool DIVERT>
 __device__ void plan_body(const U* __restrict__ src, size_t n, const ScanState* __restrict__ st,
                           const unsigned long long* ghist, unsigned long long* __restrict__ bins,
-                          Plan* __restrict__ plan, int stable, unsigned long long* __restrict__ maxb_out) {
+                          Plan* __restrict__ plan, int stable, unsigned long long* __restrict__ maxb_out,
+                          int divert) {
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
     __shared__ int live_s[ND];
@@ -326,7 +329,7 @@ __device__ void plan_body(const U* __restrict__ src, size_t n, const ScanState* 
                 }
         int skip = 0;
         if constexpr (DIVERT) {
-            if (!stable && mode == MODE_SORT) skip = skippable_digits(m, n, maxb);
+            if (divert && !stable && mode == MODE_SORT) skip = skippable_digits(m, n, maxb);
         }
         for (int i = skip; i < m; ++i) plan->pass[i - skip] = live[i];
         plan->n_live = m - skip;
