@@ -52,12 +52,14 @@ def test_segments_match_oracle(ts, t):
         assert got.tobytes() == want.tobytes(), (t, shape)
 
 
-@pytest.mark.parametrize("t", ["u32", "f32", "u64", "i16"])
-@pytest.mark.parametrize("method", [0, 1, 2])
+@pytest.mark.parametrize("t", ["u32", "f32", "u64", "i16", "i64", "f64"])
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 4])
 def test_each_method(ts, t, method):
+    """Every method in every block bin (the warp-per-segment method, 4, is for
+    the first bin only; the other bins take the MSD method with it)."""
     ctx = ts.Context(0)
     w = np.dtype(O.NP_DTYPE[t]).itemsize
-    ts.segments_methods(w, ctx, [method] * 4)
+    ts.segments_methods(w, ctx, [method] * 4 if method != 4 else [4, 3, 3, 3])
     rng = np.random.default_rng(method)
     lengths = list(rng.integers(33, 16384 if w < 8 else 8192, size=60)) + [33, 256, 257, 1024, 1025, 4096, 4097]
     a, offs = batch(t, lengths, rng)
@@ -91,12 +93,18 @@ def test_device_segments_and_graph_replay(ts):
 def test_autotune_picks_a_method_per_bin(ts):
     ctx = ts.Context(0)
     m = ts.segments_autotune(4, ctx)
-    assert len(m) == 4 and all(x in (0, 1, 2) for x in m)
+    assert len(m) == 4 and m[0] in (0, 1, 2, 3, 4) and all(x in (0, 1, 2, 3) for x in m[1:])
     rng = np.random.default_rng(9)
     a, offs = batch("u32", list(rng.integers(0, 20000, size=300)), rng)
     got = a.copy()
     ts.sort_segments(got, offs, ctx)
     assert got.tobytes() == expected(a, offs).tobytes()
+
+
+def test_warp_method_only_in_the_first_bin(ts):
+    ctx = ts.Context(0)
+    with pytest.raises(ts.TurbosortError):
+        ts.segments_methods(4, ctx, [0, 4, 0, 0])
 
 
 def test_bad_offsets_are_rejected(ts):

@@ -24,6 +24,7 @@
 
 #include "ts_common.cuh"
 #include "ts_onesweep.cuh"
+#include "ts_small.cuh"
 
 namespace ts {
 
@@ -34,7 +35,15 @@ constexpr int SEG_BIN_WARP = SEG_BLOCK_BINS;
 constexpr int SEG_BIN_LARGE = SEG_BLOCK_BINS + 1;
 constexpr int SEG_NBINS = SEG_BLOCK_BINS + 2;
 
-enum SegMethod : int { SEG_BITONIC = 0, SEG_RADIX4 = 1, SEG_RADIX8 = 2 };
+// The on-chip method of a BLOCK bin. SEG_MSD is the LARGE segments' routine
+// (one MSD pass over the key range in shared memory, run insertion sorts);
+// SEG_WARP8 (the first bin only, up to 256 keys) sorts 32 segments a CTA,
+// one a warp, eight keys a lane in registers.
+enum SegMethod : int { SEG_BITONIC = 0, SEG_RADIX4 = 1, SEG_RADIX8 = 2, SEG_MSD = 3, SEG_WARP8 = 4 };
+constexpr int SEG_METHODS = 5;
+__host__ __device__ inline bool seg_method_ok(int bin, int m) {
+    return m >= 0 && m < SEG_METHODS && (m != SEG_WARP8 || bin == 0);
+}
 
 template <typename U>
 struct SegCfg {
@@ -61,7 +70,8 @@ __host__ __device__ inline int seg_bin_of(unsigned long long len, int cap) {
 }
 
 // Work items, largest first: LARGE segments, BLOCK bins from the longest
-// down, then groups of SEG_WARPS tiny segments.
+// down (the first BLOCK bin in groups of SEG_WARPS segments when it takes
+// SEG_WARP8), then groups of SEG_WARPS tiny segments.
 __device__ __forceinline__ void seg_item(const SegPlan& p, unsigned int item, int* bin, unsigned int* first) {
     unsigned int base = 0;
     if (item < base + p.count[SEG_BIN_LARGE]) {
@@ -71,21 +81,30 @@ __device__ __forceinline__ void seg_item(const SegPlan& p, unsigned int item, in
     }
     base += p.count[SEG_BIN_LARGE];
     for (int b = SEG_BLOCK_BINS - 1; b >= 0; --b) {
-        if (item < base + p.count[b]) {
+        const bool grouped = b == 0 && p.method[0] == SEG_WARP8;
+        const unsigned int items = grouped ? (p.count[b] + SEG_WARPS - 1) / SEG_WARPS : p.count[b];
+        if (item < base + items) {
             *bin = b;
-            *first = item - base;
+            *first = grouped ? (item - base) * SEG_WARPS : item - base;
             return;
         }
-        base += p.count[b];
+        base += items;
     }
     *bin = SEG_BIN_WARP;
     *first = (item - base) * SEG_WARPS;
 }
 
-static __global__ void k_seg_items(SegPlan* plan) {
+struct SegMethods {
+    int m[SEG_BLOCK_BINS];
+};
+
+static __global__ void k_seg_items(SegPlan* plan, SegMethods methods) {
     if (threadIdx.x == 0) {
         unsigned int t = plan->count[SEG_BIN_LARGE] + (plan->count[SEG_BIN_WARP] + SEG_WARPS - 1) / SEG_WARPS;
-        for (int b = 0; b < SEG_BLOCK_BINS; ++b) t += plan->count[b];
+        for (int b = 0; b < SEG_BLOCK_BINS; ++b) {
+            plan->method[b] = methods.m[b];
+            t += b == 0 && methods.m[0] == SEG_WARP8 ? (plan->count[0] + SEG_WARPS - 1) / SEG_WARPS : plan->count[b];
+        }
         plan->items = t;
     }
 }
@@ -524,9 +543,6 @@ __device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned cha
 }
 
 // ---- the persistent launch ---------------------------------------------------
-struct SegMethods {
-    int m[SEG_BLOCK_BINS];
-};
 
 template <typename U, int XF>
 __global__ void __launch_bounds__(SEG_THREADS, 1)
@@ -559,6 +575,13 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
                 const unsigned long long b = offsets[s];
                 seg_warp_sort<U, XF>(data_in + b, data + b, (int)(offsets[s + 1] - b), lane);
             }
+        } else if (bin == 0 && methods.m[0] == SEG_WARP8) {
+            const unsigned int idx = first + warp;
+            if (idx < plan->count[0]) {
+                const unsigned int s = lists[idx];
+                const unsigned long long b = offsets[s];
+                warp_bitonic<U, XF, 8>(data_in + b, data + b, (int)(offsets[s + 1] - b), lane);
+            }
         } else {
             const unsigned int s = lists[(size_t)bin * n_seg + first];
             const unsigned long long b = offsets[s];
@@ -574,7 +597,10 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
                 }
             } else {
                 const int m = methods.m[bin];
-                if (m == SEG_BITONIC) seg_block_bitonic<U, XF>(data_in + b, data + b, len, sm);
+                if (m == SEG_MSD) {
+                    if constexpr (sizeof(U) >= 4) msd_sort<U, XF>(data_in + b, data + b, alt + b, len, smem);
+                    else seg_block_radix<U, XF, 8>(data_in + b, data + b, len, sm, cnt, warp_tot, red);
+                } else if (m == SEG_BITONIC) seg_block_bitonic<U, XF>(data_in + b, data + b, len, sm);
                 else if (m == SEG_RADIX4) seg_block_radix<U, XF, 4>(data_in + b, data + b, len, sm, cnt, warp_tot, red);
                 else seg_block_radix<U, XF, 8>(data_in + b, data + b, len, sm, cnt, warp_tot, red);
             }

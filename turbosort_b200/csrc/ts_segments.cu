@@ -70,7 +70,7 @@ ts_status seg_enqueue(ts_ctx* c, U* d, size_t n, const unsigned long long* d_off
     TS_CUDA(c, cudaMemsetAsync(base, 0, L.lists_off, c->stream));
     const int grid = (int)std::min<size_t>((n_seg + 255) / 256, (size_t)c->sm_count * 8);
     k_seg_bin_max<U, XF><<<std::max(grid, 1), 256, 0, c->stream>>>(d_off, n_seg, n, max_len, plan, lists, c->d_error);
-    k_seg_items<<<1, 32, 0, c->stream>>>(plan);
+    k_seg_items<<<1, 32, 0, c->stream>>>(plan, m);
     k_seg_sort<U, XF><<<c->sm_count, SEG_THREADS, MSD_SMEM, c->stream>>>(d, d, (U*)c->alt.p, d_off,
                                                                                      lists, n_seg, plan, counter, m);
     c->launches += 3;
@@ -265,7 +265,8 @@ ts_status autotune(ts_ctx* c) {
         cudaEventCreate(&e1);
         float best = 1e30f;
         int best_m = c->seg_methods[w][bin];
-        for (int m = SEG_BITONIC; m <= SEG_RADIX8; ++m) {
+        for (int m = 0; m < SEG_METHODS; ++m) {
+            if (!seg_method_ok(bin, m)) continue;
             c->seg_methods[w][bin] = m;
             float tot = 0.f;
             for (int rep = 0; rep < 4 && s == TS_OK; ++rep) {
@@ -316,7 +317,7 @@ ts_status ts_segments_methods(ts_ctx* c, size_t key_bytes, int* methods, int set
     const int w = width_index(key_bytes);
     for (int b = 0; b < SEG_BLOCK_BINS; ++b) {
         if (set) {
-            if (methods[b] < SEG_BITONIC || methods[b] > SEG_RADIX8) return fail(c, TS_ERR_INVALID, "unknown method");
+            if (!seg_method_ok(b, methods[b])) return fail(c, TS_ERR_INVALID, "unknown method for this bin");
             c->seg_methods[w][b] = methods[b];
         } else {
             methods[b] = c->seg_methods[w][b];

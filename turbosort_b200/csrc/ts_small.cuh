@@ -65,7 +65,8 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small_sort(const U* in, U* ou
     }
 }
 
-// One warp sorts up to 32 * R keys in registers: element e = r * 32 + lane
+// One warp sorts up to 32 * R keys in registers (warp_bitonic; k_warp_sort is
+// its launch for one slice): element e = r * 32 + lane
 // sits in register r of that lane. A bitonic network over the next power of
 // two, padded with the largest key as the crate's AVX2 tiers pad
 // (src/arch/x86_64/avx2.rs:211-313): partners 32 and more apart are in the
@@ -73,14 +74,13 @@ __global__ void __launch_bounds__(SMALL_THREADS) k_small_sort(const U* in, U* ou
 // shared memory and no block barrier: the tier for the slices the crate
 // sends to its register networks (src/tiny.rs:15, src/small.rs:11).
 template <typename U, int XF, int R>
-__global__ void __launch_bounds__(32) k_warp_sort(U* d, int n) {
+__device__ __forceinline__ void warp_bitonic(const U* in, U* out, int n, int lane) {
     constexpr int N = 32 * R;
-    const int lane = threadIdx.x;
     U v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int e = r * 32 + lane;
-        v[r] = e < n ? to_key<U, XF>(d[e]) : (U)~(U)0;
+        v[r] = e < n ? to_key<U, XF>(in[e]) : (U)~(U)0;
     }
 #pragma unroll
     for (int k = 2; k <= N; k <<= 1) {
@@ -114,8 +114,13 @@ __global__ void __launch_bounds__(32) k_warp_sort(U* d, int n) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int e = r * 32 + lane;
-        if (e < n) d[e] = from_key<U, XF>(v[r]);
+        if (e < n) out[e] = from_key<U, XF>(v[r]);
     }
+}
+
+template <typename U, int XF, int R>
+__global__ void __launch_bounds__(32) k_warp_sort(U* d, int n) {
+    warp_bitonic<U, XF, R>(d, d, n, threadIdx.x);
 }
 
 template <int XF>

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "ts_engine.cuh"
+#include "ts_segmented.cuh"
 
 namespace ts {
 namespace {
@@ -209,8 +210,8 @@ ts_status ts_ctx_tune_load(ts_ctx* c, const char* path, int* loaded) {
         for (int v : row)
             if (v < 0 || v >= LSD_VARIANTS) return fail(c, TS_ERR_INVALID, "tuning file: unknown variant");
     for (auto& row : seg)
-        for (int m : row)
-            if (m < 0 || m > 2) return fail(c, TS_ERR_INVALID, "tuning file: unknown method");
+        for (int b = 0; b < 4; ++b)
+            if (!seg_method_ok(b, row[b])) return fail(c, TS_ERR_INVALID, "tuning file: unknown method");
     const int wb[3] = {2, 4, 8};
     for (int i = 0; i < 3; ++i)
         for (int b = 0; b < LSD_BINS; ++b) c->lsd_variant[width_slot((size_t)wb[i])][b] = lsd[i][b];
