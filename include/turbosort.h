@@ -237,10 +237,11 @@ typedef struct ts_learned_params {
     int32_t use_model;       /* 0: equal-width buckets (ablation) */
     uint64_t corrupt_seed;   /* test hook, 0 = off: overwrite the trained leaves with
                                 arbitrary values before the partition (output stays exact) */
-    uint32_t route_passes;   /* cost route: when the plain sort would need at most this many
-                                scatter passes (estimated from the sample's digit histograms,
-                                diverting included; keys of at most this many bytes need no
-                                estimate), the plain sort runs instead (reason 4); 0 = never */
+    uint32_t route_passes;   /* cost route (default 4): when the plain sort would need at most
+                                this many scatter passes (estimated from the sample's digit
+                                histograms, diverting included; keys of at most this many bytes
+                                need no estimate), the plain sort runs instead (reason 4);
+                                0 = never */
     int32_t verify;          /* the judge: 1 = sort a copy with the plain LSD as well and count
                                 the keys where the outputs differ (stats->verify_mismatches);
                                 any difference returns TS_ERR_INTERNAL */

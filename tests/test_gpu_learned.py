@@ -170,14 +170,14 @@ def test_ablation_on_float_keys(ts, W, kind):
 
 def test_training_improves_the_fit(ts, W):
     """What the training gains over the same model untrained (train_iters =
-    0, heights that interpolate the sample's CDF at the breakpoints): the Adam
-    steps lower the squared rank error over all of each leaf's samples on both
-    skewed inputs (by a third or more), and on the Gaussian mixture, whose
-    modes the untrained leaves straddle, they shrink the largest bucket
-    (measured 2834 -> 2589 keys at 2^24, 45263 -> 39034 at 2^28). On the
-    lognormal input the untrained model's buckets are already as even, and on
-    neither does the bucket finish get faster: the gain is the fit and the
-    worst bucket, not time."""
+    0: heights that interpolate the sample's CDF at the breakpoints): the Adam
+    steps lower the mean squared rank error over all of each leaf's samples
+    by a third or more on both skewed inputs. That is the whole gain. The
+    buckets come out about as even either way (the largest bucket moves by a
+    few percent, down on some inputs and up on others: at 2^28 the Gaussian
+    mixture's went 2.76x -> 2.38x the mean, the lognormal's 1.77x -> 1.82x),
+    and the bucket sorts take the same time, because the untrained leaves
+    already start from the sample's quantiles."""
     for kind in ("gauss_mix_u64", "lognormal_f64"):
         a = inputs(W, kind, n=1 << 24)
         st0 = ts.sort_learned(a.copy(), train_iters=0, overflow_factor=1e9)
@@ -186,10 +186,7 @@ def test_training_improves_the_fit(ts, W):
         assert st0["train_loss_first"] == pytest.approx(st0["train_loss_last"], rel=1e-9)
         assert st1["train_loss_first"] == pytest.approx(st0["train_loss_last"], rel=1e-4)
         assert st1["train_loss_last"] < 0.75 * st1["train_loss_first"]
-        if kind == "gauss_mix_u64":
-            assert st1["max_bucket"] < 0.95 * st0["max_bucket"], (st0["max_bucket"], st1["max_bucket"])
-        else:
-            assert st1["max_bucket"] <= 1.05 * st0["max_bucket"], (st0["max_bucket"], st1["max_bucket"])
+        assert st1["max_bucket"] <= 1.1 * st0["max_bucket"], (st0["max_bucket"], st1["max_bucket"])
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
@@ -299,13 +296,14 @@ def test_full_size_equals_plain_sort(ts, W):
 
 
 @pytest.mark.parametrize("kind, n, routed", [("unit_f32_dups", N, True), ("uniform_u32", N, True),
-                                             ("uniform_u64", N, True), ("lognormal_f64", N, True),
+                                             ("uniform_u64", N, True), ("lognormal_f64", N, None),
                                              ("gauss_mix_u64", 1 << 26, False)])
 def test_cost_route(ts, W, kind, n, routed):
-    """With the default route, inputs the plain sort handles in at most five
+    """With the default route, inputs the plain sort handles in at most four
     passes take the plain sort: every 4-byte key, random 8-byte keys (which
     it diverts to four passes), and at 2^21 the lognormal f64 keys, whose top
-    digits already carry the 23 bits that diverting needs there. At 2^26 the
+    digits carry about the 23 bits that diverting needs there (routed when
+    the estimate comes to four passes or fewer). At 2^26 the
     Gaussian mixture's top digits split the keys too poorly to divert, all
     eight passes would run, and the partition takes it. The output is the
     oracle's either way."""
@@ -315,11 +313,11 @@ def test_cost_route(ts, W, kind, n, routed):
     got = a.copy()
     st = real.sort_learned(got)
     same_bits(got, O.sort_parallel(a))
-    if routed:
+    assert (st["reason"] == 4) == (0 < st["est_plain_passes"] <= 4), st
+    if routed is True:
         assert st["fell_back"] == 1 and st["reason"] == 4, st
-        assert 0 < st["est_plain_passes"] <= 5, st
-    else:
-        assert st["reason"] != 4 and st["est_plain_passes"] >= 6, st
+    elif routed is False:
+        assert st["reason"] != 4 and st["est_plain_passes"] >= 5, st
 
 
 @pytest.mark.parametrize("kind", ["lognormal_f64", "gauss_mix_u64", "unit_f32_dups", "specials_f64"])

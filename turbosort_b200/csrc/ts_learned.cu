@@ -379,9 +379,11 @@ void ts_learned_defaults(ts_learned_params* p) {
     p->max_cdf_error = 0.01f;
     p->use_model = 1;
     p->corrupt_seed = 0;
-    // measured on a B200 (2^28 keys): the partition costs about as much as six
-    // 8-byte passes, and more than four 4-byte passes
-    p->route_passes = 5;
+    // measured on a B200 (2^28 keys): the partition (8.8 ms for 8-byte keys)
+    // beats the plain sort when that needs five or more 8-byte passes
+    // (lognormal f64, diverted to five: 10.6 ms; all eight: 13.0 ms), and
+    // loses to four passes of 4-byte keys (7.1 against 4.3 ms)
+    p->route_passes = 4;
     p->verify = 0;
 }
 

@@ -5,7 +5,8 @@
 // order from a counter:
 //   1. the keys arrive in shared memory by one bulk copy (cp.async.bulk, no
 //      multicast); with two buffers (NBUF = 2) it is issued one tile ahead,
-//      with one the CTA claims its next tile early and prefetches it into L2;
+//      with one the CTA claims its next tile early, prefetches it into L2,
+//      and issues its copy as soon as this tile's keys are staged (step 4);
 //   2. a counting pass builds per-warp digit counts, the tile's
 //      digit counts are published to the look-back array at once, and the
 //      tile-local start of every (digit, warp) run is scanned;
@@ -396,6 +397,11 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
             }
         }
         __syncthreads();
+        if constexpr (NBUF == 1) {
+            // every key of this tile sits in the staging tile now: the key
+            // buffer takes the next tile's copy while this one is scattered
+            if (tid == 0 && misc[1] < a.portion_tiles) issue(misc[1], 0);
+        }
 
         // ---- 5. runs per digit to global memory (the last live pass undoes
         // the key transform as it writes)
@@ -467,32 +473,42 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
             __syncthreads();
         }
     } else {
-        // one buffer: each CTA holds the claim on its next tile while it works
-        // on this one, and brings that tile into L2 meanwhile, so the copy into
-        // shared memory that starts the next iteration reads from L2
-        if (tid == 0) misc[1] = (int)atomicAdd(a.tile_counter, 1u);
-        for (;;) {
-            if (tid == 0) {
-                const int t = misc[1];
-                misc[0] = t;
-                if (t < a.portion_tiles) {
-                    issue(t, 0);
-                    const int nx = (int)atomicAdd(a.tile_counter, 1u);
-                    misc[1] = nx;
-                    if (nx < a.portion_tiles) {
-                        const size_t nb = a.portion_begin + (size_t)nx * TILE;
-                        const size_t ne = min(portion_end, nb + TILE);
-                        prefetch_l2(src + nb, src + ne);
-                        if constexpr (PAIRS) {
-                            if (!first) prefetch_l2(vsrc + nb, vsrc + ne);
-                        }
-                    }
+        // one buffer: each CTA holds the claim on its next tile (misc[1])
+        // while it works on this one (misc[0]) and brings that tile into L2;
+        // once this tile's keys are ranked into the staging tile, the copy of
+        // the next one into the key buffer starts (in process), so it runs
+        // under this tile's look-back and scatter
+        auto claim_next = [&]() {  // thread 0
+            const int nx = (int)atomicAdd(a.tile_counter, 1u);
+            misc[1] = nx;
+            if (nx < a.portion_tiles) {
+                const size_t nb = a.portion_begin + (size_t)nx * TILE;
+                const size_t ne = min(portion_end, nb + TILE);
+                prefetch_l2(src + nb, src + ne);
+                if constexpr (PAIRS) {
+                    if (!first) prefetch_l2(vsrc + nb, vsrc + ne);
                 }
             }
-            __syncthreads();
+        };
+        if (tid == 0) {
+            const int t = (int)atomicAdd(a.tile_counter, 1u);
+            misc[0] = t;
+            if (t < a.portion_tiles) {
+                issue(t, 0);
+                claim_next();
+            }
+        }
+        __syncthreads();
+        for (;;) {
             const int t = misc[0];
             if (t >= a.portion_tiles) break;
             run_tile(t, 0);
+            __syncthreads();
+            if (tid == 0) {
+                const int t2 = misc[1];  // its copy was issued by run_tile
+                misc[0] = t2;
+                if (t2 < a.portion_tiles) claim_next();
+            }
             __syncthreads();
         }
     }
