@@ -113,3 +113,29 @@ def test_bad_offsets_are_rejected(ts):
         ts.sort_segments(a, np.array([0, 5, 3], dtype=np.uint64))
     with pytest.raises(ts.TurbosortError):
         ts.sort_segments(a, np.array([0, 11], dtype=np.uint64))
+
+
+@pytest.mark.parametrize("t", ["u32", "f32", "i64", "u64", "f64"])
+def test_segments_above_the_on_chip_capacity(ts, t):
+    """Segments of up to eight times the shared-memory MSD capacity (49.6K
+    4-byte or 24.8K 8-byte keys) are cut by key range into parts that fit;
+    a part whose narrow key range alone holds too many keys takes the CTA
+    LSD. Shapes: random keys, keys crowded into one tiny range with a few
+    outliers, two distinct values, and every key equal, at lengths around
+    the capacity and its multiples."""
+    w = np.dtype(O.NP_DTYPE[t]).itemsize
+    cap = 49_600 if w == 4 else 24_800
+    rng = np.random.default_rng(77)
+    lengths = [cap - 1, cap + 1, 2 * cap + 3, 5 * cap, 8 * cap - 5, 8 * cap + 9, 70_000, 150_000]
+    a, offs = batch(t, lengths, rng)
+    k = a.view(O.KEY_DTYPE[t])
+    lo, hi = int(offs[1]), int(offs[2])            # crowded: 99% of the keys in a 1000-wide range
+    k[lo:hi] = np.where(rng.random(hi - lo) < 0.99, rng.integers(0, 1000, size=hi - lo),
+                        rng.integers(0, 2**31, size=hi - lo)).astype(k.dtype)
+    lo, hi = int(offs[2]), int(offs[3])            # two values
+    k[lo:hi] = np.where(rng.random(hi - lo) < 0.5, 3, 12345).astype(k.dtype)
+    lo, hi = int(offs[3]), int(offs[4])            # every key equal
+    k[lo:hi] = 42
+    got = a.copy()
+    ts.sort_segments(got, offs)
+    assert got.tobytes() == expected(a, offs).tobytes()

@@ -410,7 +410,7 @@ struct MsdSmem {
 // One segment, by the whole CTA (1024 threads); `sm` is MSD_SMEM bytes of
 // shared memory; `scratch` has room for len keys.
 template <typename U, int XF>
-__device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
+__device__ void msd_core(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
     using M = MsdSmem<U>;
     U* sk = reinterpret_cast<U*>(sm);
     unsigned int* wd = reinterpret_cast<unsigned int*>(sm + M::words);  // counter d: half (d & 1) of wd[d >> 1]
@@ -540,6 +540,155 @@ __device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned cha
     __syncthreads();
     for (int i = tid; i < len; i += 1024) dst[i] = from_key<U, XF>(sk[i]);
     __syncthreads();
+}
+
+// Segments of up to MSD_SPLIT_PARTS times the on-chip capacity: one coarse
+// MSD pass cuts the key range into 4096 equal sub-ranges, consecutive
+// sub-ranges are grouped into parts of at most the capacity (one sub-range
+// that alone holds more is a part of its own), the keys go to their part in
+// `scratch` (placed by sub-range), and each part is copied to its place in
+// dst and sorted there: on chip by msd_core, or, when one narrow key range
+// holds more keys than fit, by the CTA-level LSD through its own stretch of
+// scratch. The parts are in key order, so the segment ends up sorted.
+constexpr int MSD_SPLIT_PARTS = 8;
+constexpr int MSD_COARSE = 4096;
+constexpr int MSD_MAX_PARTS = 128;  // the greedy grouping makes at most 2 * MSD_SPLIT_PARTS + 1
+
+template <typename U, int XF>
+__device__ void msd_split(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
+    using M = MsdSmem<U>;
+    uint32_t* cur = reinterpret_cast<uint32_t*>(sm);                 // [MSD_COARSE] counts, then cursors
+    uint32_t* cnt = cur + MSD_COARSE;                                // [MSD_COARSE] counts
+    int* misc = reinterpret_cast<int*>(sm + M::misc);
+    int* warp_tot = misc;                                            // [32]
+    unsigned long long* red = reinterpret_cast<unsigned long long*>(misc + 32);  // [4]
+    int* bounds = misc + 64;                                         // [MSD_MAX_PARTS + 1] part starts, then len
+    int* nparts = misc + 64 + MSD_MAX_PARTS + 1;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // the key range
+    if (tid == 0) {
+        red[0] = ~0ull;
+        red[1] = 0ull;
+    }
+    for (int i = tid; i < MSD_COARSE; i += 1024) cur[i] = 0u;
+    __syncthreads();
+    unsigned long long mn = ~0ull, mx = 0ull;
+    msd_for_keys<U>(src, len, [&](int, U v) {
+        const unsigned long long k = (unsigned long long)to_key<U, XF>(v);
+        mn = k < mn ? k : mn;
+        mx = k > mx ? k : mx;
+    });
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, mn, o);
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, mx, o);
+        mn = x < mn ? x : mn;
+        mx = y > mx ? y : mx;
+    }
+    if (lane == 0) {
+        atomicMin(&red[0], mn);
+        atomicMax(&red[1], mx);
+    }
+    __syncthreads();
+    const unsigned long long kmin = red[0], kmax = red[1];
+    if (kmin == kmax) {  // every key equal
+        msd_for_keys<U>(src, len, [&](int i, U v) { dst[i] = v; });
+        __syncthreads();
+        return;
+    }
+    const float scale = (float)MSD_COARSE / __ull2float_ru(kmax - kmin);
+    auto coarse = [&](U v) {
+        return min(MSD_COARSE - 1, (int)(__ull2float_rz((unsigned long long)to_key<U, XF>(v) - kmin) * scale));
+    };
+    msd_for_keys<U>(src, len, [&](int, U v) { atomicAdd(&cur[coarse(v)], 1u); });
+    __syncthreads();
+    // exclusive scan (four sub-ranges a thread); counts kept for the grouping
+    uint32_t c4[4], sum = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        c4[q] = cur[tid * 4 + q];
+        sum += c4[q];
+    }
+    uint32_t x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = (int)x;
+    __syncthreads();
+    uint32_t run = x - sum;
+    for (int w = 0; w < warp; ++w) run += (uint32_t)warp_tot[w];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        cnt[tid * 4 + q] = c4[q];
+        cur[tid * 4 + q] = run;
+        run += c4[q];
+    }
+    __syncthreads();
+    // parts: greedy groups of consecutive sub-ranges of at most cap keys
+    // (thread 0 reads only the counts: the other threads move the cursors meanwhile)
+    if (tid == 0) {
+        int np = 0, acc = 0, off = 0;
+        bool ok = true;
+        bounds[0] = 0;
+        for (int i = 0; i < MSD_COARSE; ++i) {
+            const int ci = (int)cnt[i];
+            if (acc > 0 && acc + ci > M::cap) {
+                if (np + 1 >= MSD_MAX_PARTS) {
+                    ok = false;
+                    break;
+                }
+                bounds[++np] = off;
+                acc = 0;
+            }
+            acc += ci;
+            off += ci;
+        }
+        bounds[++np] = len;
+        *nparts = ok ? np : -1;
+    }
+    // place every key in its part of scratch (by sub-range)
+    msd_for_keys<U>(src, len, [&](int, U v) { scratch[atomicAdd(&cur[coarse(v)], 1u)] = v; });
+    __syncthreads();
+    const int np = *nparts;
+    if (np < 0) {  // cannot happen (see MSD_MAX_PARTS); the CTA-level LSD takes the segment
+        uint32_t* l_cnt = reinterpret_cast<uint32_t*>(sm + (size_t)SegCfg<U>::LARGE_TILE * sizeof(U));
+        uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
+        uint32_t* l_run = l_hist + 8 * 256;
+        for (int i = tid; i < len; i += 1024) dst[i] = scratch[i];
+        __syncthreads();
+        seg_large_sort<U, XF>(dst, dst, scratch, len, reinterpret_cast<U*>(sm), l_cnt, warp_tot, &red[3], l_hist,
+                              l_run, l_run + 256, l_run + 512);
+        __syncthreads();
+        return;
+    }
+    int part_bounds[2];
+    for (int p = 0; p < np; ++p) {
+        part_bounds[0] = bounds[p];
+        part_bounds[1] = bounds[p + 1];
+        __syncthreads();  // every thread has its bounds before the part reuses shared memory
+        const int a = part_bounds[0], plen = part_bounds[1] - part_bounds[0];
+        for (int i = tid; i < plen; i += 1024) dst[a + i] = scratch[a + i];
+        __syncthreads();
+        if (plen <= M::cap) {
+            msd_core<U, XF>(dst + a, dst + a, scratch + a, plen, sm);
+        } else {
+            uint32_t* l_cnt = reinterpret_cast<uint32_t*>(sm + (size_t)SegCfg<U>::LARGE_TILE * sizeof(U));
+            uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
+            uint32_t* l_run = l_hist + 8 * 256;
+            seg_large_sort<U, XF>(dst + a, dst + a, scratch + a, plen, reinterpret_cast<U*>(sm), l_cnt, warp_tot,
+                                  &red[3], l_hist, l_run, l_run + 256, l_run + 512);
+        }
+        __syncthreads();
+    }
+}
+
+// One segment, by the whole CTA (1024 threads); `sm` is MSD_SMEM bytes of
+// shared memory; `scratch` has room for len keys and is not src or dst
+// (src may equal dst).
+template <typename U, int XF>
+__device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
+    if (len > MsdSmem<U>::cap && len <= MSD_SPLIT_PARTS * MsdSmem<U>::cap) msd_split<U, XF>(src, dst, scratch, len, sm);
+    else msd_core<U, XF>(src, dst, scratch, len, sm);
 }
 
 // ---- the persistent launch ---------------------------------------------------
