@@ -430,13 +430,39 @@ def bench_by_key(ts, torch, ctx, lg, steps, warmup, peak):
             "ok": ok, "checks": "sorted, stable (equal keys keep input order), permutation, records and side slice moved"}
 
 
-def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True):
+def bench_tiny(ts, torch, ctx, steps):
+    """Latency of one plain device sort of a short slice (the crate's tiny
+    and small tiers, src/tiny.rs, src/small.rs): median CUDA-event time of a
+    single call, same buffer each time."""
+    out = {}
+    for n in (17, 100, 256, 1000, 4096):
+        host = np.random.default_rng(n).integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+        master = torch.from_numpy(host.view(np.int32)).to(f"cuda:{ctx.device}")
+        d = torch.empty_like(master)
+        times = []
+        for i in range(steps + 3):
+            d.copy_(master)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ts.sort(d.view(torch.uint32), ctx)
+            e1.record()
+            torch.cuda.synchronize()
+            if i >= 3:
+                times.append(e0.elapsed_time(e1))
+        ok = check_exact(d.cpu().numpy().view(np.uint32), expected_radix(host))
+        out[str(n)] = {"us": round(1000 * statistics.median(times), 2), "ok": ok}
+    return out
+
+
+def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True, count=100_000):
     """Config 4: 100,000 segments with lengths log-uniform on [1, 65536], keys
     of random bits, sorted in one segmented launch (graph replay, autotuned
     on-chip methods), against one plain sort call per segment."""
     from turbosort_b200 import workloads as W
 
-    lengths = W.segment_lengths(100_000)
+    lengths = W.segment_lengths(count)
     offs = np.zeros(lengths.size + 1, dtype=np.uint64)
     offs[1:] = np.cumsum(lengths)
     n = int(offs[-1])
@@ -475,6 +501,7 @@ def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True):
     del packed
     ok = check_exact(out, want)
     res = {"gkeys_s": round(n / (ms / 1e3) / 1e9, 3), "ms": round(ms, 3), "keys": n, "segments": int(lengths.size),
+           "methods_names": ["bitonic", "radix-4", "radix-8", "msd", "warp"],
            "methods_per_bin": methods, "ok": ok,
            "roofline_frac": round(2 * n * 4 / (ms / 1e3) / 1e9 / measured_peak_gbs()[0], 3)}
     if per_segment:
@@ -593,6 +620,9 @@ def main() -> None:
     ap.add_argument("--learned", default=None, choices=["lognormal_f64", "gauss_mix_u64", "unit_f32_dups"],
                     help="only the learned-partition comparison on this input (2^log2n keys, default 2^28)")
     ap.add_argument("--buckets-log2", type=int, default=14, help="buckets of the learned partition (with --learned)")
+    ap.add_argument("--segments", default=None, choices=["u32", "f32"],
+                    help="only the segmented-sort comparison (config 4) for these keys")
+    ap.add_argument("--segment-count", type=int, default=100_000, help="segments (with --segments)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -609,6 +639,18 @@ def main() -> None:
         res = bench_learned(ts, torch, ctx, args.learned, args.steps, args.warmup, measured_peak_gbs()[0],
                             lg=args.log2n or 28, buckets_log2=args.buckets_log2)
         print(json.dumps({"learned": args.learned, **res}), flush=True)
+        return
+
+    if args.segments:
+        import torch
+
+        import turbosort_b200 as ts
+
+        ctx = ts.Context(0)
+        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        res = bench_segments(ts, torch, ctx, args.segments, args.steps, args.warmup, per_segment=False,
+                             count=args.segment_count)
+        print(json.dumps({"segments": args.segments, **res}), flush=True)
         return
 
     import torch
@@ -633,6 +675,11 @@ def main() -> None:
     kind, dist, lg = WORKLOADS[args.workload]
     if args.log2n:
         lg = args.log2n
+    # the tile autotuner for the workload's key width (and 8-byte keys for the
+    # breakdown), before anything is timed
+    tuning = {str(WIDTH[kind]): ctx.lsd_autotune(WIDTH[kind])}
+    if not args.no_breakdown and WIDTH[kind] != 8:
+        tuning["8"] = ctx.lsd_autotune(8)
     clocks = Clocks(local)
     clocks.start()
     r = bench_device(ts, torch, ctx, kind, dist, lg, args.steps, args.warmup, 0x9E3779B97F4A7C15 + rank, dist_mod,
@@ -673,6 +720,7 @@ def main() -> None:
         "kernel_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in r["timings"].items()},
         "gpu_launches": int(r["launches"]),
         "clocks": clk,
+        "tuning": tuning,
     }
 
     # end to end through the host-slice C ABI call, pinned host memory: the
@@ -753,6 +801,7 @@ def main() -> None:
                         "pass_frac": round(rr["n"] * rr["w"] * 2 / (ow / 1e3) / 1e9 / peak, 3) if ow else None,
                         "ok": rr["ok"]}
         bd["c1_u32_2p20"] = bench_small(ts, torch, ctx, "u32", 0, 20, max(10, args.steps), 5, 0x1234 + rank)
+        bd["tiny_slices_u32"] = bench_tiny(ts, torch, ctx, max(10, args.steps))
         bd["c3_by_key_zipf_u64_2p27"] = bench_by_key(ts, torch, ctx, 27, max(3, args.steps // 2), 3, peak)
         for kind in ("u32", "f32"):
             bd[f"c4_segments_{kind}"] = bench_segments(ts, torch, ctx, kind, max(3, args.steps // 2), 2)
