@@ -38,6 +38,8 @@ struct LsdCfg {
     // the first live pass of a keys-only sort ranks with shared atomics
     // (k_onesweep, UNSTABLE1)
     static constexpr bool UNSTABLE1 = true;
+    // the next item's equals found before this item's counter update (k_onesweep)
+    static constexpr bool RANK_AHEAD = false;
     // 8-byte keys without positions divert (src/radix/divert.rs): the plan may
     // leave out the lowest live digits, and k_divert_runs / k_divert_long
     // finish the runs that leaves
@@ -159,9 +161,9 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         using Sm = typename C::Smem;
         auto kern = n <= (size_t)0x7fffffff
                         ? k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1>
+                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD>
                         : k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1>;
+                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD>;
         const int occ = occupancy(c, kern, C::THREADS, Sm::bytes);
         SweepArgs<U, PAIRS> a{};
         a.in = in;

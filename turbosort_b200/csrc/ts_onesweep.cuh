@@ -119,7 +119,7 @@ struct PeerMasks {
 // equal in every bit are the same bit pattern, so their order is not
 // observable. With positions (PAIRS) every pass stays stable.
 template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
-          int MATCH_CNT, bool UNSTABLE1 = false>
+          int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<U, PAIRS> a) {
     using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
     using OFF = typename std::conditional<BIG, long long, int>::type;
@@ -319,6 +319,36 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                     const U k = load_key(kb[idx]);
                     sk[atomicAdd(&my_cnt[dig(k)], 1u)] = k;
                 }
+            }
+        } else if constexpr (RANK_AHEAD) {
+            // ---- 3. as below, with the equals of item i + 1 found (ballots
+            // and shuffles only, no memory) before item i's counter update,
+            // so that the two overlap
+            auto find = [&](int i, U& k, uint32_t& d, uint32_t& peers) {
+                const int idx = wbase + i * 32;
+                k = load_key(kb[FULL ? idx : min(idx, TILE - 1)]);
+                d = dig(k);
+                if ((i % MATCH_MOD) < MATCH_CNT) peers = __match_any_sync(0xffffffffu, d);
+                else peers = pm.peers(d);
+                if (!FULL) peers &= __ballot_sync(0xffffffffu, idx < tile_n);
+            };
+            U kn;
+            uint32_t dn, pn;
+            find(0, kn, dn, pn);
+#pragma unroll
+            for (int i = 0; i < IPT; ++i) {
+                const int idx = wbase + i * 32;
+                const U k = kn;
+                const uint32_t d = dn, peers = pn;
+                if (i + 1 < IPT) find(i + 1, kn, dn, pn);
+                if (FULL || idx < tile_n) {
+                    const uint32_t c = my_cnt[d];
+                    my_cnt[d] = c + __popc(peers);
+                    const uint32_t pos = c + __popc(peers & lt);
+                    sk[pos] = k;
+                    if constexpr (PAIRS) sv[pos] = FIRST ? (uint32_t)(tile_base + idx) : vb[idx];
+                }
+                __syncwarp();
             }
         } else {
             // ---- 3. rank among equal digits in the warp and stage in sorted order
