@@ -40,6 +40,8 @@ struct LsdCfg {
     static constexpr bool UNSTABLE1 = true;
     // the next item's equals found before this item's counter update (k_onesweep)
     static constexpr bool RANK_AHEAD = false;
+    // look-back entries loaded per round trip
+    static constexpr int LBW = LB_WINDOW;
     // 8-byte keys without positions divert (src/radix/divert.rs): the plan may
     // leave out the lowest live digits, and k_divert_runs / k_divert_long
     // finish the runs that leaves
@@ -161,9 +163,9 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         using Sm = typename C::Smem;
         auto kern = n <= (size_t)0x7fffffff
                         ? k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD>
+                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW>
                         : k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD>;
+                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW>;
         const int occ = occupancy(c, kern, C::THREADS, Sm::bytes);
         SweepArgs<U, PAIRS> a{};
         a.in = in;

@@ -119,7 +119,7 @@ struct PeerMasks {
 // equal in every bit are the same bit pattern, so their order is not
 // observable. With positions (PAIRS) every pass stays stable.
 template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
-          int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false>
+          int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false, int LBW = LB_WINDOW>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<U, PAIRS> a) {
     using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
     using OFF = typename std::conditional<BIG, long long, int>::type;
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                 const int r = tid * DPT + q;
                 uint32_t excl = 0;
                 if (t > 0) {
-                    // LB_WINDOW predecessors per round trip: their loads go out
+                    // LBW predecessors per round trip: their loads go out
                     // together, then they are summed newest first up to the
                     // first inclusive entry; an entry not yet published ends
                     // the round there and the next round starts from it
@@ -390,14 +390,14 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                     uint32_t spins = 0;
                     bool done = false;
                     while (j >= 0 && !done) {
-                        uint32_t w[LB_WINDOW];
+                        uint32_t w[LBW];
 #pragma unroll
-                        for (int k = 0; k < LB_WINDOW; ++k)
+                        for (int k = 0; k < LBW; ++k)
                             w[k] = j - k >= 0 ? ld_relaxed_gpu(a.lookback + (size_t)(j - k) * RADIX + r) : LB_FLAG_INC;
                         int adv = 0;
                         bool stalled = false;
 #pragma unroll
-                        for (int k = 0; k < LB_WINDOW; ++k) {
+                        for (int k = 0; k < LBW; ++k) {
                             const uint32_t f = w[k] & ~LB_VALUE;
                             if (done || stalled) continue;
                             if (f == 0) {
