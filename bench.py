@@ -456,7 +456,7 @@ def bench_tiny(ts, torch, ctx, steps):
     return out
 
 
-def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True, count=100_000):
+def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True, count=100_000, tune=True):
     """Config 4: 100,000 segments with lengths log-uniform on [1, 65536], keys
     of random bits, sorted in one segmented launch (graph replay, autotuned
     on-chip methods), against one plain sort call per segment."""
@@ -469,7 +469,7 @@ def bench_segments(ts, torch, ctx, kind, steps, warmup, per_segment=True, count=
     bits = W.plain_u32(n, seed=0x2545F4914F6CDD1D)
     host = bits.view(np.float32) if kind == "f32" else bits
     dev = f"cuda:{ctx.device}"
-    methods = ts.segments_autotune(4, ctx)
+    methods = ts.segments_autotune(4, ctx) if tune else ts.segments_methods(4, ctx)
     master = torch.from_numpy(bits.view(np.int32)).to(dev)
     d = torch.empty_like(master)
     d_off = torch.from_numpy(offs.view(np.int64)).to(dev)
@@ -620,6 +620,8 @@ def main() -> None:
     ap.add_argument("--learned", default=None, choices=["lognormal_f64", "gauss_mix_u64", "unit_f32_dups"],
                     help="only the learned-partition comparison on this input (2^log2n keys, default 2^28)")
     ap.add_argument("--buckets-log2", type=int, default=14, help="buckets of the learned partition (with --learned)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the tile autotuner (the library's measured defaults; for profiling runs)")
     ap.add_argument("--segments", default=None, choices=["u32", "f32"],
                     help="only the segmented-sort comparison (config 4) for these keys")
     ap.add_argument("--segment-count", type=int, default=100_000, help="segments (with --segments)")
@@ -649,7 +651,7 @@ def main() -> None:
         ctx = ts.Context(0)
         ctx.set_stream(torch.cuda.current_stream().cuda_stream)
         res = bench_segments(ts, torch, ctx, args.segments, args.steps, args.warmup, per_segment=False,
-                             count=args.segment_count)
+                             count=args.segment_count, tune=not args.no_tune)
         print(json.dumps({"segments": args.segments, **res}), flush=True)
         return
 
@@ -677,9 +679,12 @@ def main() -> None:
         lg = args.log2n
     # the tile autotuner for the workload's key width (and 8-byte keys for the
     # breakdown), before anything is timed
-    tuning = {str(WIDTH[kind]): ctx.lsd_autotune(WIDTH[kind])}
-    if not args.no_breakdown and WIDTH[kind] != 8:
-        tuning["8"] = ctx.lsd_autotune(8)
+    if args.no_tune:
+        tuning = {str(WIDTH[kind]): {"variants": ctx.lsd_variants(WIDTH[kind]), "tuned": False}}
+    else:
+        tuning = {str(WIDTH[kind]): ctx.lsd_autotune(WIDTH[kind])}
+        if not args.no_breakdown and WIDTH[kind] != 8:
+            tuning["8"] = ctx.lsd_autotune(8)
     clocks = Clocks(local)
     clocks.start()
     r = bench_device(ts, torch, ctx, kind, dist, lg, args.steps, args.warmup, 0x9E3779B97F4A7C15 + rank, dist_mod,

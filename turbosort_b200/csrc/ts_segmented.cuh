@@ -408,7 +408,8 @@ struct MsdSmem {
 };
 
 // One segment, by the whole CTA (1024 threads); `sm` is MSD_SMEM bytes of
-// shared memory; `scratch` has room for len keys.
+// shared memory; `scratch` has room for len keys, or is null when src may be
+// overwritten (it then serves as the CTA LSD's second buffer).
 template <typename U, int XF>
 __device__ void msd_core(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
     using M = MsdSmem<U>;
@@ -510,8 +511,17 @@ __device__ void msd_core(const U* src, U* dst, U* scratch, int len, unsigned cha
         if (tid == 0) red[2] = 0ull;
     }
     if (large) {
-        seg_large_sort<U, XF>(src, dst, scratch, len, sk, l_cnt, warp_tot, &red[3], l_hist, l_run, l_run + 256,
-                              l_run + 512);
+        if (scratch == nullptr) {
+            // src is expendable (msd_split's parts): sort in dst, with src as
+            // the LSD's second buffer
+            for (int i = tid; i < len; i += 1024) dst[i] = src[i];
+            __syncthreads();
+            seg_large_sort<U, XF>(dst, dst, const_cast<U*>(src), len, sk, l_cnt, warp_tot, &red[3], l_hist, l_run,
+                                  l_run + 256, l_run + 512);
+        } else {
+            seg_large_sort<U, XF>(src, dst, scratch, len, sk, l_cnt, warp_tot, &red[3], l_hist, l_run, l_run + 256,
+                                  l_run + 512);
+        }
         __syncthreads();
         return;
     }
@@ -543,32 +553,35 @@ __device__ void msd_core(const U* src, U* dst, U* scratch, int len, unsigned cha
 }
 
 // Segments of up to MSD_SPLIT_PARTS times the on-chip capacity: one coarse
-// MSD pass cuts the key range into 4096 equal sub-ranges, consecutive
-// sub-ranges are grouped into parts of at most the capacity (one sub-range
-// that alone holds more is a part of its own), the keys go to their part in
-// `scratch` (placed by sub-range), and each part is copied to its place in
-// dst and sorted there: on chip by msd_core, or, when one narrow key range
-// holds more keys than fit, by the CTA-level LSD through its own stretch of
-// scratch. The parts are in key order, so the segment ends up sorted.
-constexpr int MSD_SPLIT_PARTS = 8;
+// MSD pass cuts the key range into MSD_COARSE equal sub-ranges; with T the
+// capacity less the fullest sub-range, sub-range r goes to part start_r / T
+// (start_r: keys in the sub-ranges before it), so every part holds at most
+// the capacity unless one narrow key range alone holds more; the keys go to
+// their part in `scratch` (each warp groups its keys by part, so a part's keys
+// from one warp land at consecutive addresses), and each part is sorted from
+// there into its place in dst: by msd_core, whose CTA-level LSD takes a part
+// too crowded for the sub-range pass. The parts are in key order, so the
+// segment ends up sorted.
+constexpr int MSD_SPLIT_PARTS = 4;
 constexpr int MSD_COARSE = 4096;
-constexpr int MSD_MAX_PARTS = 128;  // the greedy grouping makes at most 2 * MSD_SPLIT_PARTS + 1
+constexpr int MSD_MAX_PARTS = 16;  // ceil(len / T) with T >= len / 16
 
 template <typename U, int XF>
 __device__ void msd_split(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
     using M = MsdSmem<U>;
-    uint32_t* cur = reinterpret_cast<uint32_t*>(sm);                 // [MSD_COARSE] counts, then cursors
-    uint32_t* cnt = cur + MSD_COARSE;                                // [MSD_COARSE] counts
+    uint32_t* cur = reinterpret_cast<uint32_t*>(sm);                       // [MSD_COARSE] counts, then starts
+    unsigned char* part_of = sm + MSD_COARSE * 4;                          // [MSD_COARSE]
     int* misc = reinterpret_cast<int*>(sm + M::misc);
-    int* warp_tot = misc;                                            // [32]
+    int* warp_tot = misc;                                                  // [32]
     unsigned long long* red = reinterpret_cast<unsigned long long*>(misc + 32);  // [4]
-    int* bounds = misc + 64;                                         // [MSD_MAX_PARTS + 1] part starts, then len
-    int* nparts = misc + 64 + MSD_MAX_PARTS + 1;
+    int* bounds = misc + 64;                                               // [MSD_MAX_PARTS + 1]
+    int* pcur = misc + 64 + MSD_MAX_PARTS + 1;                             // [MSD_MAX_PARTS]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // the key range
     if (tid == 0) {
         red[0] = ~0ull;
         red[1] = 0ull;
+        red[2] = 0ull;
     }
     for (int i = tid; i < MSD_COARSE; i += 1024) cur[i] = 0u;
     __syncthreads();
@@ -601,83 +614,69 @@ __device__ void msd_split(const U* src, U* dst, U* scratch, int len, unsigned ch
     };
     msd_for_keys<U>(src, len, [&](int, U v) { atomicAdd(&cur[coarse(v)], 1u); });
     __syncthreads();
-    // exclusive scan (four sub-ranges a thread); counts kept for the grouping
-    uint32_t c4[4], sum = 0;
+    // exclusive scan (four sub-ranges a thread) and the fullest sub-range
+    uint32_t c4[4], sum = 0, mc = 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         c4[q] = cur[tid * 4 + q];
         sum += c4[q];
+        mc = max(mc, c4[q]);
     }
     uint32_t x = sum;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
+    for (int o = 16; o > 0; o >>= 1) mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
     if (lane == 31) warp_tot[warp] = (int)x;
+    if (lane == 0) atomicMax(reinterpret_cast<unsigned int*>(&red[2]), mc);
+    if (tid <= MSD_MAX_PARTS) bounds[tid] = len;
     __syncthreads();
     uint32_t run = x - sum;
     for (int w = 0; w < warp; ++w) run += (uint32_t)warp_tot[w];
+    const int maxc = (int)reinterpret_cast<unsigned int*>(&red[2])[0];
+    const int target = max(M::cap - maxc, (len + MSD_MAX_PARTS - 1) / MSD_MAX_PARTS);
+    // sub-range r's part, and each part's first key (a part that receives
+    // no sub-range starts where the next one does)
+    int prev_part = -1;
+    if (tid > 0)  // the part of the previous thread's last sub-range
+        prev_part = min(MSD_MAX_PARTS - 1, (int)((run - cur[tid * 4 - 1]) / (uint32_t)target));
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        cnt[tid * 4 + q] = c4[q];
-        cur[tid * 4 + q] = run;
+        const int p = min(MSD_MAX_PARTS - 1, (int)(run / (uint32_t)target));
+        part_of[tid * 4 + q] = (unsigned char)p;
+        if (p != prev_part) atomicMin(&bounds[p], (int)run);
+        prev_part = p;
         run += c4[q];
     }
     __syncthreads();
-    // parts: greedy groups of consecutive sub-ranges of at most cap keys
-    // (thread 0 reads only the counts: the other threads move the cursors meanwhile)
     if (tid == 0) {
-        int np = 0, acc = 0, off = 0;
-        bool ok = true;
+        for (int p = MSD_MAX_PARTS - 1; p >= 0; --p) bounds[p] = min(bounds[p], bounds[p + 1]);
         bounds[0] = 0;
-        for (int i = 0; i < MSD_COARSE; ++i) {
-            const int ci = (int)cnt[i];
-            if (acc > 0 && acc + ci > M::cap) {
-                if (np + 1 >= MSD_MAX_PARTS) {
-                    ok = false;
-                    break;
-                }
-                bounds[++np] = off;
-                acc = 0;
-            }
-            acc += ci;
-            off += ci;
-        }
-        bounds[++np] = len;
-        *nparts = ok ? np : -1;
+        for (int p = 0; p < MSD_MAX_PARTS; ++p) pcur[p] = bounds[p];
     }
-    // place every key in its part of scratch (by sub-range)
-    msd_for_keys<U>(src, len, [&](int, U v) { scratch[atomicAdd(&cur[coarse(v)], 1u)] = v; });
     __syncthreads();
-    const int np = *nparts;
-    if (np < 0) {  // cannot happen (see MSD_MAX_PARTS); the CTA-level LSD takes the segment
-        uint32_t* l_cnt = reinterpret_cast<uint32_t*>(sm + (size_t)SegCfg<U>::LARGE_TILE * sizeof(U));
-        uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
-        uint32_t* l_run = l_hist + 8 * 256;
-        for (int i = tid; i < len; i += 1024) dst[i] = scratch[i];
-        __syncthreads();
-        seg_large_sort<U, XF>(dst, dst, scratch, len, reinterpret_cast<U*>(sm), l_cnt, warp_tot, &red[3], l_hist,
-                              l_run, l_run + 256, l_run + 512);
-        __syncthreads();
-        return;
+    // place the keys by part: a warp's keys of one part at consecutive places
+    PeerMasks<4> pm;
+    pm.init(lane);
+    const uint32_t lt = lanemask_lt();
+    for (int base = warp * 32; base < len; base += 1024) {  // warp-uniform
+        const int i = base + lane;
+        const bool valid = i < len;
+        const U v = valid ? src[i] : (U)0;
+        const uint32_t p = valid ? part_of[coarse(v)] : 0u;
+        const uint32_t peers = pm.peers(p) & __ballot_sync(0xffffffffu, valid);
+        const int leader = __ffs(peers) - 1;
+        uint32_t at = 0;
+        if (valid && lane == leader) at = (uint32_t)atomicAdd(&pcur[p], __popc(peers));
+        at = __shfl_sync(0xffffffffu, at, leader & 31);
+        if (valid) scratch[at + __popc(peers & lt)] = v;
     }
-    int part_bounds[2];
-    for (int p = 0; p < np; ++p) {
-        part_bounds[0] = bounds[p];
-        part_bounds[1] = bounds[p + 1];
-        __syncthreads();  // every thread has its bounds before the part reuses shared memory
-        const int a = part_bounds[0], plen = part_bounds[1] - part_bounds[0];
-        for (int i = tid; i < plen; i += 1024) dst[a + i] = scratch[a + i];
-        __syncthreads();
-        if (plen <= M::cap) {
-            msd_core<U, XF>(dst + a, dst + a, scratch + a, plen, sm);
-        } else {
-            uint32_t* l_cnt = reinterpret_cast<uint32_t*>(sm + (size_t)SegCfg<U>::LARGE_TILE * sizeof(U));
-            uint32_t* l_hist = l_cnt + SEG_WARPS * 256;
-            uint32_t* l_run = l_hist + 8 * 256;
-            seg_large_sort<U, XF>(dst + a, dst + a, scratch + a, plen, reinterpret_cast<U*>(sm), l_cnt, warp_tot,
-                                  &red[3], l_hist, l_run, l_run + 256, l_run + 512);
-        }
+    __syncthreads();
+    for (int p = 0; p < MSD_MAX_PARTS; ++p) {
+        const int a = bounds[p], b = bounds[p + 1];
+        __syncthreads();  // every thread has the bounds before the part reuses shared memory
+        if (b > a) msd_core<U, XF>(scratch + a, dst + a, nullptr, b - a, sm);
         __syncthreads();
     }
 }
@@ -687,7 +686,8 @@ __device__ void msd_split(const U* src, U* dst, U* scratch, int len, unsigned ch
 // (src may equal dst).
 template <typename U, int XF>
 __device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned char* sm) {
-    if (len > MsdSmem<U>::cap && len <= MSD_SPLIT_PARTS * MsdSmem<U>::cap) msd_split<U, XF>(src, dst, scratch, len, sm);
+    if (len > MsdSmem<U>::cap && len <= MSD_SPLIT_PARTS * MsdSmem<U>::cap)
+        msd_split<U, XF>(src, dst, scratch, len, sm);
     else msd_core<U, XF>(src, dst, scratch, len, sm);
 }
 
