@@ -44,6 +44,8 @@ struct LsdCfg {
     static constexpr bool RANK_AHEAD = true;
     // look-back entries loaded per round trip
     static constexpr int LBW = LB_WINDOW;
+    // two threads walk each digit's look-back (k_onesweep LB_PAIR)
+    static constexpr bool LB_PAIR = false;
     // 8-byte keys without positions divert (src/radix/divert.rs): the plan may
     // leave out the lowest live digits, and k_divert_runs / k_divert_long
     // finish the runs that leaves
@@ -165,9 +167,9 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         using Sm = typename C::Smem;
         auto kern = n <= (size_t)0x7fffffff
                         ? k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW>
+                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>
                         : k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW>;
+                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>;
         const int occ = occupancy(c, kern, C::THREADS, Sm::bytes);
         SweepArgs<U, PAIRS> a{};
         a.in = in;

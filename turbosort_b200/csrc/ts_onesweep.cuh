@@ -67,7 +67,8 @@ struct SweepSmem {
     static constexpr size_t sv_off = al(sk_off + (size_t)TILE * sizeof(U));           // [TILE] u32 sorted
     static constexpr size_t cnt_off = al(sv_off + (PAIRS ? (size_t)TILE * 4 : 0));    // [RANK_WARPS][RADIX] u32
     static constexpr size_t gbase_off = al(cnt_off + (size_t)RANK_WARPS * RADIX * 4);  // [RADIX] i64
-    static constexpr size_t bar_off = al(gbase_off + (size_t)RADIX * 8);              // [2] mbarrier
+    static constexpr size_t lbc_off = al(gbase_off + (size_t)RADIX * 8);              // [RADIX] u32 x2: counts, starts
+    static constexpr size_t bar_off = al(lbc_off + (size_t)RADIX * 8);                // [2] mbarrier
     static constexpr size_t misc_off = bar_off + 16;                                  // ints
     static constexpr size_t bytes = misc_off + 4 * 64;
     static_assert(TILE * sizeof(U) % 16 == 0, "bulk copies move multiples of 16 bytes");
@@ -119,7 +120,7 @@ struct PeerMasks {
 // equal in every bit are the same bit pattern, so their order is not
 // observable. With positions (PAIRS) every pass stays stable.
 template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
-          int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false, int LBW = LB_WINDOW>
+          int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false, int LBW = LB_WINDOW, bool LB_PAIR = false>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<U, PAIRS> a) {
     using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
     using OFF = typename std::conditional<BIG, long long, int>::type;
@@ -152,6 +153,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
     U* sk = reinterpret_cast<U*>(smem + L::sk_off);
     uint32_t* sv = reinterpret_cast<uint32_t*>(smem + L::sv_off);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(smem + L::cnt_off);
+    uint32_t* lb_cnt = reinterpret_cast<uint32_t*>(smem + L::lbc_off);  // LB_PAIR: each digit's tile count
+    uint32_t* lb_start = lb_cnt + RADIX;                                // and tile-local start
     OFF* gbase = reinterpret_cast<OFF*>(smem + L::gbase_off);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::bar_off);
     int* misc = reinterpret_cast<int*>(smem + L::misc_off);  // [0..2] tile ids, [32..] warp totals
@@ -303,6 +306,10 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
             for (int q = 0; q < DPT; ++q) {
                 const int r = tid * DPT + q;
                 lstart[q] = run;
+                if constexpr (LB_PAIR) {
+                    lb_cnt[r] = tcount[q];
+                    lb_start[r] = run;
+                }
 #pragma unroll
                 for (int w = 0; w < RANK_WARPS; ++w) cnt[w * RADIX + r] += run;
                 run += tcount[q];
@@ -376,7 +383,76 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
         // ---- 4. owners: keys of their digit in earlier tiles (the decoupled
         // look-back; predecessors have had the whole ranking pass to publish),
         // then the digit's global base
-        if (tid < OWNERS) {
+        if constexpr (LB_PAIR) {
+            // two adjacent threads a digit: each loads LBW predecessors, the
+            // pair covers 2 x LBW per round trip; the even thread publishes
+            static_assert(2 * RADIX == THREADS && DPT == 1, "a pair of threads per digit");
+            const int r = tid >> 1, h = tid & 1;
+            const uint32_t pair = 3u << (lane & ~1);
+            const uint32_t tc = lb_cnt[r];
+            uint32_t excl = 0;
+            if (t > 0) {
+                int j = t - 1;
+                uint32_t spins = 0;
+                bool done = false;
+                while (j >= 0 && !done) {
+                    uint32_t w[LBW];
+#pragma unroll
+                    for (int k = 0; k < LBW; ++k) {
+                        const int e = j - h * LBW - k;
+                        w[k] = e >= 0 ? ld_relaxed_gpu(a.lookback + (size_t)e * RADIX + r) : LB_FLAG_INC;
+                    }
+                    int adv = 0;
+                    uint32_t sum = 0;
+                    bool stop = false, inc = false;
+#pragma unroll
+                    for (int k = 0; k < LBW; ++k) {
+                        const uint32_t f = w[k] & ~LB_VALUE;
+                        if (stop) continue;
+                        if (f == 0) {
+                            stop = true;
+                            continue;
+                        }
+                        sum += w[k] & LB_VALUE;
+                        ++adv;
+                        if (f == LB_FLAG_INC) stop = inc = true;
+                    }
+                    // the older half counts only when the newer half was all aggregates
+                    const int adv1 = __shfl_xor_sync(pair, adv, 1);
+                    const uint32_t sum1 = __shfl_xor_sync(pair, sum, 1);
+                    const int inc1 = __shfl_xor_sync(pair, (int)inc, 1);
+                    const int adv0 = h ? adv1 : adv, adv_o = h ? adv : adv1;
+                    const uint32_t sum0 = h ? sum1 : sum, sum_o = h ? sum : sum1;
+                    const bool inc0 = h ? inc1 != 0 : inc, inc_o = h ? inc : inc1 != 0;
+                    int step = adv0;
+                    uint32_t add = sum0;
+                    bool fin = inc0;
+                    if (adv0 == LBW && !inc0) {
+                        step += adv_o;
+                        add += sum_o;
+                        fin = inc_o;
+                    }
+                    excl += add;
+                    j -= step;
+                    done = fin;
+                    if (step == 0 && ++spins > a.spin_limit) {
+                        if (h == 0) atomicOr(a.error, ERR_TIMEOUT);
+                        break;
+                    }
+                }
+                if (h == 0) st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, LB_FLAG_INC | (excl + tc));
+            }
+            if (h == 0) {
+                const unsigned long long carry = a.carry_in ? a.carry_in[r] : 0ull;
+                unsigned long long start = bins[r] + carry + excl;
+                if (start + tc > a.n) {  // only after a timeout: keep every write in bounds
+                    atomicOr(a.error, ERR_BOUNDS);
+                    start = a.n - tc;
+                }
+                gbase[r] = (OFF)((long long)start - (long long)lb_start[r]);
+                if (a.carry_out && t == a.portion_tiles - 1) a.carry_out[r] = carry + excl + tc;
+            }
+        } else if (tid < OWNERS) {
 #pragma unroll
             for (int q = 0; q < DPT; ++q) {
                 const int r = tid * DPT + q;
