@@ -53,13 +53,16 @@ def test_segments_match_oracle(ts, t):
 
 
 @pytest.mark.parametrize("t", ["u32", "f32", "u64", "i16", "i64", "f64"])
-@pytest.mark.parametrize("method", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 4, 5])
 def test_each_method(ts, t, method):
-    """Every method in every block bin (the warp-per-segment method, 4, is for
-    the first bin only; the other bins take the MSD method with it)."""
+    """Every method in every block bin (the warp-per-segment methods are for
+    the first bin, 4, and for the second with keys of up to 4 bytes, 5; the
+    other bins take the MSD method with them)."""
     ctx = ts.Context(0)
     w = np.dtype(O.NP_DTYPE[t]).itemsize
-    ts.segments_methods(w, ctx, [method] * 4 if method != 4 else [4, 3, 3, 3])
+    if method == 5 and w > 4:
+        pytest.skip("the 32-keys-a-lane warp method takes keys of up to 4 bytes")
+    ts.segments_methods(w, ctx, {4: [4, 3, 3, 3], 5: [4, 5, 3, 3]}.get(method, [method] * 4))
     rng = np.random.default_rng(method)
     lengths = list(rng.integers(33, 16384 if w < 8 else 8192, size=60)) + [33, 256, 257, 1024, 1025, 4096, 4097]
     a, offs = batch(t, lengths, rng)
@@ -93,7 +96,7 @@ def test_device_segments_and_graph_replay(ts):
 def test_autotune_picks_a_method_per_bin(ts):
     ctx = ts.Context(0)
     m = ts.segments_autotune(4, ctx)
-    assert len(m) == 4 and m[0] in (0, 1, 2, 3, 4) and all(x in (0, 1, 2, 3) for x in m[1:])
+    assert len(m) == 4 and m[0] in (0, 1, 2, 3, 4) and m[1] in (0, 1, 2, 3, 5) and all(x in (0, 1, 2, 3) for x in m[2:])
     rng = np.random.default_rng(9)
     a, offs = batch("u32", list(rng.integers(0, 20000, size=300)), rng)
     got = a.copy()
@@ -101,10 +104,11 @@ def test_autotune_picks_a_method_per_bin(ts):
     assert got.tobytes() == expected(a, offs).tobytes()
 
 
-def test_warp_method_only_in_the_first_bin(ts):
+def test_warp_methods_only_in_their_bins(ts):
     ctx = ts.Context(0)
-    with pytest.raises(ts.TurbosortError):
-        ts.segments_methods(4, ctx, [0, 4, 0, 0])
+    for bad, w in (([0, 4, 0, 0], 4), ([5, 0, 0, 0], 4), ([0, 0, 5, 0], 4), ([0, 5, 0, 0], 8)):
+        with pytest.raises(ts.TurbosortError):
+            ts.segments_methods(w, ctx, bad)
 
 
 def test_bad_offsets_are_rejected(ts):

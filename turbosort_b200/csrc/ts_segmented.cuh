@@ -37,12 +37,19 @@ constexpr int SEG_NBINS = SEG_BLOCK_BINS + 2;
 
 // The on-chip method of a BLOCK bin. SEG_MSD is the LARGE segments' routine
 // (one MSD pass over the key range in shared memory, run insertion sorts);
-// SEG_WARP8 (the first bin only, up to 256 keys) sorts 32 segments a CTA,
-// one a warp, eight keys a lane in registers.
-enum SegMethod : int { SEG_BITONIC = 0, SEG_RADIX4 = 1, SEG_RADIX8 = 2, SEG_MSD = 3, SEG_WARP8 = 4 };
-constexpr int SEG_METHODS = 5;
-__host__ __device__ inline bool seg_method_ok(int bin, int m) {
-    return m >= 0 && m < SEG_METHODS && (m != SEG_WARP8 || bin == 0);
+// SEG_WARP8 (the first bin, up to 256 keys) and SEG_WARP32 (the second bin,
+// up to 1024 keys of at most 4 bytes) sort 32 segments a CTA, one a warp, in
+// registers (8 or 32 keys a lane; 16 when a segment has at most 512).
+enum SegMethod : int { SEG_BITONIC = 0, SEG_RADIX4 = 1, SEG_RADIX8 = 2, SEG_MSD = 3, SEG_WARP8 = 4, SEG_WARP32 = 5 };
+constexpr int SEG_METHODS = 6;
+__host__ __device__ inline bool seg_method_ok(int bin, int m, int key_bytes) {
+    if (m < 0 || m >= SEG_METHODS) return false;
+    if (m == SEG_WARP8) return bin == 0;
+    if (m == SEG_WARP32) return bin == 1 && key_bytes <= 4;
+    return true;
+}
+__host__ __device__ inline bool seg_grouped(int bin, int m) {
+    return (bin == 0 && m == SEG_WARP8) || (bin == 1 && m == SEG_WARP32);
 }
 
 template <typename U>
@@ -81,7 +88,7 @@ __device__ __forceinline__ void seg_item(const SegPlan& p, unsigned int item, in
     }
     base += p.count[SEG_BIN_LARGE];
     for (int b = SEG_BLOCK_BINS - 1; b >= 0; --b) {
-        const bool grouped = b == 0 && p.method[0] == SEG_WARP8;
+        const bool grouped = seg_grouped(b, p.method[b]);
         const unsigned int items = grouped ? (p.count[b] + SEG_WARPS - 1) / SEG_WARPS : p.count[b];
         if (item < base + items) {
             *bin = b;
@@ -103,7 +110,7 @@ static __global__ void k_seg_items(SegPlan* plan, SegMethods methods) {
         unsigned int t = plan->count[SEG_BIN_LARGE] + (plan->count[SEG_BIN_WARP] + SEG_WARPS - 1) / SEG_WARPS;
         for (int b = 0; b < SEG_BLOCK_BINS; ++b) {
             plan->method[b] = methods.m[b];
-            t += b == 0 && methods.m[0] == SEG_WARP8 ? (plan->count[0] + SEG_WARPS - 1) / SEG_WARPS : plan->count[b];
+            t += seg_grouped(b, methods.m[b]) ? (plan->count[b] + SEG_WARPS - 1) / SEG_WARPS : plan->count[b];
         }
         plan->items = t;
     }
@@ -724,12 +731,18 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
                 const unsigned long long b = offsets[s];
                 seg_warp_sort<U, XF>(data_in + b, data + b, (int)(offsets[s + 1] - b), lane);
             }
-        } else if (bin == 0 && methods.m[0] == SEG_WARP8) {
+        } else if (seg_grouped(bin, methods.m[bin])) {
             const unsigned int idx = first + warp;
-            if (idx < plan->count[0]) {
-                const unsigned int s = lists[idx];
+            if (idx < plan->count[bin]) {
+                const unsigned int s = lists[(size_t)bin * n_seg + idx];
                 const unsigned long long b = offsets[s];
-                warp_bitonic<U, XF, 8>(data_in + b, data + b, (int)(offsets[s + 1] - b), lane);
+                const int len = (int)(offsets[s + 1] - b);
+                if (bin == 0 || len <= 512) {
+                    if (bin == 0) warp_bitonic<U, XF, 8>(data_in + b, data + b, len, lane);
+                    else warp_bitonic<U, XF, 16>(data_in + b, data + b, len, lane);
+                } else if constexpr (sizeof(U) <= 4) {
+                    warp_bitonic<U, XF, 32>(data_in + b, data + b, len, lane);
+                }
             }
         } else {
             const unsigned int s = lists[(size_t)bin * n_seg + first];

@@ -266,7 +266,7 @@ ts_status autotune(ts_ctx* c) {
         float best = 1e30f;
         int best_m = c->seg_methods[w][bin];
         for (int m = 0; m < SEG_METHODS; ++m) {
-            if (!seg_method_ok(bin, m)) continue;
+            if (!seg_method_ok(bin, m, (int)sizeof(U))) continue;
             c->seg_methods[w][bin] = m;
             float tot = 0.f;
             for (int rep = 0; rep < 4 && s == TS_OK; ++rep) {
@@ -317,7 +317,8 @@ ts_status ts_segments_methods(ts_ctx* c, size_t key_bytes, int* methods, int set
     const int w = width_index(key_bytes);
     for (int b = 0; b < SEG_BLOCK_BINS; ++b) {
         if (set) {
-            if (!seg_method_ok(b, methods[b])) return fail(c, TS_ERR_INVALID, "unknown method for this bin");
+            if (!seg_method_ok(b, methods[b], (int)key_bytes))
+                return fail(c, TS_ERR_INVALID, "unknown method for this bin and key width");
             c->seg_methods[w][b] = methods[b];
         } else {
             methods[b] = c->seg_methods[w][b];

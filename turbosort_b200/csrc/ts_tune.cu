@@ -209,9 +209,10 @@ ts_status ts_ctx_tune_load(ts_ctx* c, const char* path, int* loaded) {
     for (auto& row : lsd)
         for (int v : row)
             if (v < 0 || v >= LSD_VARIANTS) return fail(c, TS_ERR_INVALID, "tuning file: unknown variant");
-    for (auto& row : seg)
+    const int sbytes[4] = {1, 2, 4, 8};
+    for (int i = 0; i < 4; ++i)
         for (int b = 0; b < 4; ++b)
-            if (!seg_method_ok(b, row[b])) return fail(c, TS_ERR_INVALID, "tuning file: unknown method");
+            if (!seg_method_ok(b, seg[i][b], sbytes[i])) return fail(c, TS_ERR_INVALID, "tuning file: unknown method");
     const int wb[3] = {2, 4, 8};
     for (int i = 0; i < 3; ++i)
         for (int b = 0; b < LSD_BINS; ++b) c->lsd_variant[width_slot((size_t)wb[i])][b] = lsd[i][b];
