@@ -47,7 +47,7 @@ struct ts_ctx {
     // plain LSD: the tile variant (k_onesweep keys a thread, halved per step)
     // per key width (1, 2, 4, 8 bytes) and length bin (< 2^22, < 2^25, more),
     // set by ts_lsd_autotune; the defaults were measured on a B200
-    int lsd_variant[4][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}};
+    int lsd_variant[4][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 0}, {0, 0, 0}};
     // segmented sort: the method of each on-chip length bin per key width
     // (1, 2, 4, 8 bytes), set by the autotuner; and the last captured graph
     int seg_methods[4][4] = {{4, 5, 2, 2}, {4, 5, 2, 2}, {4, 5, 3, 3}, {4, 3, 3, 3}};
