@@ -2,9 +2,11 @@
 //
 // The tier choice follows the crate's dispatcher (src/dispatch.rs:31-111):
 // n <= 1 is a no-op; one-byte keys take the counting sort
-// (src/radix/mod.rs:123-164); short slices take the bitonic tiers
-// (src/tiny.rs, src/small.rs: one warp in registers up to 256 keys, one CTA
-// in shared memory up to 4096); the rest runs the LSD
+// (src/radix/mod.rs:123-164); short slices take the on-chip tiers
+// (src/tiny.rs, src/small.rs: one warp's register bitonic network up to 256
+// keys, and up to 1024 keys of 4 bytes or 512 of 8; then one CTA, by the MSD
+// routine for 4- and 8-byte keys and a shared-memory bitonic network for
+// 1- and 2-byte keys, up to 4096); the rest runs the LSD
 // passes (src/radix/mod.rs:180-271). The presorted early-out
 // (src/presorted.rs:15-65) and the constant-digit skip are decided on the
 // device, so nothing in a sort waits on the host.
@@ -239,6 +241,20 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
             k_warp_sort<U, XF, 1><<<1, 32, 0, c->stream>>>(d_data, (int)n);
         } else if (n <= (size_t)WARP_TIER_MAX) {
             k_warp_sort<U, XF, WARP_TIER_MAX / 32><<<1, 32, 0, c->stream>>>(d_data, (int)n);
+        } else if (n <= 512 && sizeof(U) == 8) {
+            k_warp_sort<U, XF, 16><<<1, 32, 0, c->stream>>>(d_data, (int)n);
+        } else if (n <= 1024 && sizeof(U) <= 4) {
+            k_warp_sort<U, XF, 32><<<1, 32, 0, c->stream>>>(d_data, (int)n);
+        } else if constexpr (sizeof(U) >= 4) {
+            // the one-CTA MSD routine; its CTA-level LSD fallback (keys crowding
+            // one sub-range) needs a second buffer of n keys
+            ts_status s;
+            if (!d_alt) {
+                if ((s = grow(c, c->alt, n * sizeof(U), "scratch keys")) != TS_OK) return s;
+                d_alt = (U*)c->alt.p;
+            }
+            occupancy_of((const void*)k_msd_slice<U, XF>, SEG_THREADS, MSD_SMEM);
+            k_msd_slice<U, XF><<<1, SEG_THREADS, MSD_SMEM, c->stream>>>(d_data, d_alt, (int)n);
         } else {
             const int threads = (int)std::min<size_t>(SMALL_THREADS, std::max<size_t>(32, (n + 1) / 2));
             k_small_sort<U, XF, false><<<1, threads, 0, c->stream>>>(d_data, d_data, nullptr, (int)n, 1);

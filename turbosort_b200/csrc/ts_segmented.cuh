@@ -698,6 +698,16 @@ __device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned cha
     else msd_core<U, XF>(src, dst, scratch, len, sm);
 }
 
+// One slice of up to 4096 keys of 4 or 8 bytes by one CTA: the plain sort's
+// short-slice tier above the warp networks (src/small.rs:11 sorts up to 512
+// with its networks; here the one-pass MSD routine takes 1025..4096 keys, a
+// few barriers instead of the bitonic network's 78 stages).
+template <typename U, int XF>
+__global__ void __launch_bounds__(SEG_THREADS, 1) k_msd_slice(U* d, U* __restrict__ scratch, int n) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    msd_sort<U, XF>(d, d, scratch, n, smem);
+}
+
 // ---- the persistent launch ---------------------------------------------------
 
 template <typename U, int XF>
