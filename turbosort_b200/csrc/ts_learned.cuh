@@ -869,7 +869,7 @@ __global__ void __launch_bounds__(1024, 1) k_lm_finish(const U* __restrict__ in,
             item_s[0] = item_s[1];
             const int nb = (int)atomicAdd(counter, 1u);
             item_s[1] = nb;
-            if (nb < buckets) prefetch_l2(in + offsets[nb], in + offsets[nb + 1]);
+            if (nb < buckets) prefetch_l2(in + offsets[nb], in + min(offsets[nb + 1], offsets[nb] + (1ull << 22)));
         }
         __syncthreads();
         const int b = item_s[0];

@@ -725,8 +725,27 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
     int* item_s = misc + 40;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned int items = plan->items;
+    // thread 0 holds the claim on the CTA's next item and brings a single
+    // segment's keys into L2 while this item is sorted (the sorts run from
+    // shared memory and L2, so their first read no longer waits on DRAM)
+    unsigned int next = 0;
+    if (threadIdx.x == 0) next = atomicAdd(counter, 1u);
     for (;;) {
-        if (threadIdx.x == 0) *item_s = (int)atomicAdd(counter, 1u);
+        if (threadIdx.x == 0) {
+            *item_s = (int)next;
+            next = atomicAdd(counter, 1u);
+            if (next < items) {
+                int nbin;
+                unsigned int nfirst;
+                seg_item(*plan, next, &nbin, &nfirst);
+                if (nbin != SEG_BIN_WARP && !(nbin < SEG_BLOCK_BINS && seg_grouped(nbin, methods.m[nbin]))) {
+                    const unsigned int s = lists[(size_t)nbin * n_seg + nfirst];
+                    const unsigned long long b = offsets[s];
+                    const unsigned long long e = min(offsets[s + 1], b + (1ull << 22));  // at most 16-32 MB
+                    prefetch_l2(data_in + b, data_in + e);
+                }
+            }
+        }
         __syncthreads();
         const unsigned int item = (unsigned int)*item_s;
         __syncthreads();
