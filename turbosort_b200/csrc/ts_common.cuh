@@ -157,6 +157,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
     return false;
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start before its predecessor in the stream has finished;
+// dep_wait() blocks until that predecessor has completed and its writes are
+// visible (a no-op for an ordinary launch), and dep_release() lets the next
+// such kernel start launching early. Every kernel of the LSD chain calls
+// dep_wait() before it touches memory.
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void dep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

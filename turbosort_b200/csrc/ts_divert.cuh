@@ -110,6 +110,8 @@ __global__ void __launch_bounds__(256, 4) k_divert_runs(const Plan* __restrict__
                                                      unsigned long long* __restrict__ runs,
                                                      unsigned long long* __restrict__ n_runs, size_t runs_cap,
                                                      uint32_t* __restrict__ error, int vec_ok) {
+    dep_wait();
+    dep_release();
     if (plan->mode != MODE_SORT || plan->divert_shift <= 0) return;
     constexpr int KPT = 32 / sizeof(U);  // two 16-byte vectors
     constexpr int W = 32 * KPT;          // keys a warp step
@@ -171,6 +173,8 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
     k_divert_long(const Plan* __restrict__ plan, U* d, U* __restrict__ alt, size_t n,
                   const unsigned long long* __restrict__ runs, const unsigned long long* __restrict__ n_runs,
                   unsigned int* __restrict__ counter, uint32_t* __restrict__ error) {
+    dep_wait();
+    dep_release();
     if (plan->mode != MODE_SORT || plan->divert_shift <= 0) return;
     extern __shared__ __align__(128) unsigned char smem[];
     // the last 16 bytes of the launch's shared memory, which msd_sort leaves alone

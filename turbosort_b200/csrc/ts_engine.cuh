@@ -118,6 +118,25 @@ static int occupancy(ts_ctx*, K kernel, int threads, size_t smem) {
 }
 
 static inline bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+// A launch on the context's stream that may begin while the previous kernel
+// in the stream finishes (programmatic stream serialization): the kernel
+// calls dep_wait() before it reads or writes anything, so only the launch
+// latency overlaps.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_dep(ts_ctx* c, void (*kernel)(KArgs...), int grid, int block, size_t smem, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 // row of the per-width tuning tables: 1, 2, 4, 8 bytes
 static inline int width_slot(size_t bytes) { return bytes == 1 ? 0 : bytes == 2 ? 1 : bytes == 4 ? 2 : 3; }
 
@@ -162,9 +181,8 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
         static_assert(144 + 8 * ND <= 256, "the plan area holds every digit's largest bucket");
         auto kern = k_hist<U, XF, C::BITS, T, C::DIVERT>;
         const int occ = occupancy(c, kern, T, smem);
-        kern<<<c->sm_count * occ, T, smem, c->stream>>>(in, n, st, hist, vec_ok, bins, plan, PAIRS ? 1 : 0,
-                                                         (unsigned long long*)(meta + m.maxb_off()),
-                                                         c->divert ? 1 : 0);
+        TS_CUDA(c, launch_dep(c, kern, c->sm_count * occ, T, smem, in, n, st, hist, vec_ok, bins, plan, PAIRS ? 1 : 0,
+                              (unsigned long long*)(meta + m.maxb_off()), c->divert ? 1 : 0));
         ++c->launches;
     }
     {
@@ -203,7 +221,7 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
                 a.withhold_tile0 = c->test_spin_limit != 0 && launch == 0;
                 const int grid = (int)std::min((size_t)c->sm_count * occ, (size_t)a.portion_tiles);
                 mark(c, "onesweep");
-                kern<<<grid, C::THREADS, Sm::bytes, c->stream>>>(a);
+                TS_CUDA(c, launch_dep(c, kern, grid, C::THREADS, Sm::bytes, a));
                 ++c->launches;
             }
         }
@@ -293,7 +311,8 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
             if (st != TS_OK) return st;
             mark(c, "finish");
             const int grid = c->sm_count * 4;
-            k_finish_keys<U><<<grid, 512, 0, c->stream>>>(plan, d_alt, d_data, n, aligned16(d_alt) && aligned16(d_data));
+            TS_CUDA(c, launch_dep(c, k_finish_keys<U>, grid, 512, 0, (const Plan*)plan, (const U*)d_alt, d_data, n,
+                                  (int)(aligned16(d_alt) && aligned16(d_data))));
             ++c->launches;
             if constexpr (DIVERT) {
                 const MetaLayout m = MetaLayout::make(LsdCfg<U, false>::ND, LsdCfg<U, false>::RADIX, 0);

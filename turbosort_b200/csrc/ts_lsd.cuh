@@ -51,6 +51,7 @@ template <typename U, int XF, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_scan(const U* __restrict__ src, size_t n, int bits, int nd,
                                                   ScanState* __restrict__ st, int vec_ok, uint4* __restrict__ lb,
                                                   size_t lb_vecs) {
+    dep_release();  // the histogram kernel may launch early (it waits for this one)
     // the first onesweep launch's look-back region starts at zero (each
     // launch clears the next one's); done before any warp can leave
     for (size_t i = (size_t)blockIdx.x * THREADS + threadIdx.x; i < lb_vecs; i += (size_t)gridDim.x * THREADS)
@@ -164,6 +165,8 @@ __global__ void __launch_bounds__(THREADS) k_hist(const U* __restrict__ src, siz
                                                   unsigned long long* __restrict__ bins, Plan* __restrict__ plan,
                                                   int stable, unsigned long long* __restrict__ maxb_out,
                                                   int divert) {
+    dep_wait();
+    dep_release();
     static_assert(THREADS >= 32 * ((Bits<U>::W + BITS - 1) / BITS), "the plan scans a digit a warp");
     constexpr int RADIX = 1 << BITS;
     constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
@@ -347,6 +350,8 @@ __device__ void plan_body(const U* __restrict__ src, size_t n, const ScanState* 
 // input (src/presorted.rs:15-65), as the plan says; nothing otherwise.
 template <typename U>
 __global__ void k_finish_keys(const Plan* __restrict__ plan, const U* from, U* to, size_t n, int vec_ok) {
+    dep_wait();
+    dep_release();
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     if (plan->mode == MODE_REVERSE) {
         for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 2; i += stride) {
@@ -370,6 +375,8 @@ __global__ void k_finish_keys(const Plan* __restrict__ plan, const U* from, U* t
 }
 
 static __global__ void k_iota_if_unsorted(const Plan* __restrict__ plan, uint32_t* __restrict__ order, size_t n) {
+    dep_wait();
+    dep_release();
     if (plan->mode == MODE_SORT && plan->n_live > 0) return;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) order[i] = (uint32_t)i;
