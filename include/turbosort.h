@@ -186,7 +186,9 @@ TS_DECLARE_SEGMENTS(f64, double)
  * 4-bit digits, 2 radix with 8-bit digits, 3 one MSD pass over the key range
  * in shared memory then insertion sorts of the short sub-range runs, 4 (first
  * bin only) one warp a segment, eight keys a lane in registers, 5 (second bin,
- * keys of up to 4 bytes) one warp a segment, 16 or 32 keys a lane. ts_segments_autotune times every
+ * keys of up to 4 bytes) one warp a segment, 16 or 32 keys a lane, 6 (third and
+ * fourth bins, keys of 4 and 8 bytes) the MSD pass by thread groups, four or
+ * two segments a CTA at once. ts_segments_autotune times every
  * method on synthetic batches of each bin on this GPU and keeps the fastest;
  * ts_segments_methods reads (set = 0) or sets (set = 1) the four methods. */
 ts_status ts_segments_autotune(ts_ctx *ctx, size_t key_bytes);

@@ -53,16 +53,19 @@ def test_segments_match_oracle(ts, t):
 
 
 @pytest.mark.parametrize("t", ["u32", "f32", "u64", "i16", "i64", "f64"])
-@pytest.mark.parametrize("method", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 4, 5, 6])
 def test_each_method(ts, t, method):
-    """Every method in every block bin (the warp-per-segment methods are for
-    the first bin, 4, and for the second with keys of up to 4 bytes, 5; the
-    other bins take the MSD method with them)."""
+    """Every method in every block bin it serves: the warp-per-segment
+    methods in the first bin (4) and, for keys of up to 4 bytes, the second
+    (5); the grouped MSD method (6) in the third and fourth, for keys of 4 and
+    8 bytes. Bins a method does not serve take the MSD method meanwhile."""
     ctx = ts.Context(0)
     w = np.dtype(O.NP_DTYPE[t]).itemsize
     if method == 5 and w > 4:
         pytest.skip("the 32-keys-a-lane warp method takes keys of up to 4 bytes")
-    ts.segments_methods(w, ctx, {4: [4, 3, 3, 3], 5: [4, 5, 3, 3]}.get(method, [method] * 4))
+    if method == 6 and w < 4:
+        pytest.skip("the grouped MSD method takes keys of 4 and 8 bytes")
+    ts.segments_methods(w, ctx, {4: [4, 3, 3, 3], 5: [4, 5, 3, 3], 6: [4, 3, 6, 6]}.get(method, [method] * 4))
     rng = np.random.default_rng(method)
     lengths = list(rng.integers(33, 16384 if w < 8 else 8192, size=60)) + [33, 256, 257, 1024, 1025, 4096, 4097]
     a, offs = batch(t, lengths, rng)
@@ -96,7 +99,7 @@ def test_device_segments_and_graph_replay(ts):
 def test_autotune_picks_a_method_per_bin(ts):
     ctx = ts.Context(0)
     m = ts.segments_autotune(4, ctx)
-    assert len(m) == 4 and m[0] in (0, 1, 2, 3, 4) and m[1] in (0, 1, 2, 3, 5) and all(x in (0, 1, 2, 3) for x in m[2:])
+    assert len(m) == 4 and m[0] in (0, 1, 2, 3, 4) and m[1] in (0, 1, 2, 3, 5) and all(x in (0, 1, 2, 3, 6) for x in m[2:])
     rng = np.random.default_rng(9)
     a, offs = batch("u32", list(rng.integers(0, 20000, size=300)), rng)
     got = a.copy()
@@ -106,7 +109,8 @@ def test_autotune_picks_a_method_per_bin(ts):
 
 def test_warp_methods_only_in_their_bins(ts):
     ctx = ts.Context(0)
-    for bad, w in (([0, 4, 0, 0], 4), ([5, 0, 0, 0], 4), ([0, 0, 5, 0], 4), ([0, 5, 0, 0], 8)):
+    for bad, w in (([0, 4, 0, 0], 4), ([5, 0, 0, 0], 4), ([0, 0, 5, 0], 4), ([0, 5, 0, 0], 8), ([0, 6, 0, 0], 4),
+                   ([0, 0, 6, 0], 2)):
         with pytest.raises(ts.TurbosortError):
             ts.segments_methods(w, ctx, bad)
 

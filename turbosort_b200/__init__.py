@@ -443,7 +443,8 @@ def segments_methods(key_bytes: int, ctx: Context | None = None, methods=None) -
     """Read (or set) the on-chip method of each segment length bin for keys of
     `key_bytes`: 0 bitonic, 1 radix with 4-bit digits, 2 radix with 8-bit digits,
     3 one MSD pass in shared memory, 4 (first bin only) one warp a segment, 5 (second bin,
-    keys of up to 4 bytes) one warp a segment, 16 or 32 keys a lane."""
+    keys of up to 4 bytes) one warp a segment, 16 or 32 keys a lane, 6 (third and fourth
+    bins, 4- and 8-byte keys) the MSD pass by thread groups, several segments a CTA."""
     ctx = ctx or default_context(0)
     arr = (ctypes.c_int * 4)(*(methods or [0, 0, 0, 0]))
     ctx._check(lib().ts_segments_methods(ctx.handle, key_bytes, arr, 1 if methods is not None else 0))

@@ -50,7 +50,7 @@ struct ts_ctx {
     int lsd_variant[4][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 0}, {0, 0, 0}};
     // segmented sort: the method of each on-chip length bin per key width
     // (1, 2, 4, 8 bytes), set by the autotuner; and the last captured graph
-    int seg_methods[4][4] = {{4, 5, 2, 2}, {4, 5, 2, 2}, {4, 5, 3, 3}, {4, 3, 3, 3}};
+    int seg_methods[4][4] = {{4, 5, 2, 2}, {4, 5, 2, 2}, {4, 5, 6, 6}, {4, 3, 6, 6}};
     bool use_graphs = true;
     bool capturing = false;
     cudaGraphExec_t seg_graph = nullptr;

@@ -40,17 +40,27 @@ constexpr int SEG_NBINS = SEG_BLOCK_BINS + 2;
 // SEG_WARP8 (the first bin, up to 256 keys) and SEG_WARP32 (the second bin,
 // up to 1024 keys of at most 4 bytes) sort 32 segments a CTA, one a warp, in
 // registers (8 or 32 keys a lane; 16 when a segment has at most 512).
-enum SegMethod : int { SEG_BITONIC = 0, SEG_RADIX4 = 1, SEG_RADIX8 = 2, SEG_MSD = 3, SEG_WARP8 = 4, SEG_WARP32 = 5 };
-constexpr int SEG_METHODS = 6;
+// SEG_MSD_GROUPS (the third and fourth bins, keys of 4 and 8 bytes) runs the
+// MSD routine in thread groups, four segments a CTA in the third bin (up to
+// 4096 keys) and two in the fourth.
+enum SegMethod : int {
+    SEG_BITONIC = 0, SEG_RADIX4 = 1, SEG_RADIX8 = 2, SEG_MSD = 3, SEG_WARP8 = 4, SEG_WARP32 = 5, SEG_MSD_GROUPS = 6
+};
+constexpr int SEG_METHODS = 7;
 __host__ __device__ inline bool seg_method_ok(int bin, int m, int key_bytes) {
     if (m < 0 || m >= SEG_METHODS) return false;
     if (m == SEG_WARP8) return bin == 0;
     if (m == SEG_WARP32) return bin == 1 && key_bytes <= 4;
+    if (m == SEG_MSD_GROUPS) return (bin == 2 || bin == 3) && key_bytes >= 4;
     return true;
 }
-__host__ __device__ inline bool seg_grouped(int bin, int m) {
-    return (bin == 0 && m == SEG_WARP8) || (bin == 1 && m == SEG_WARP32);
+// segments a work item of this bin and method takes
+__host__ __device__ inline int seg_per_item(int bin, int m) {
+    if ((bin == 0 && m == SEG_WARP8) || (bin == 1 && m == SEG_WARP32)) return SEG_WARPS;
+    if (m == SEG_MSD_GROUPS) return bin == 2 ? 4 : 2;
+    return 1;
 }
+__host__ __device__ inline bool seg_grouped(int bin, int m) { return seg_per_item(bin, m) > 1; }
 
 template <typename U>
 struct SegCfg {
@@ -88,11 +98,11 @@ __device__ __forceinline__ void seg_item(const SegPlan& p, unsigned int item, in
     }
     base += p.count[SEG_BIN_LARGE];
     for (int b = SEG_BLOCK_BINS - 1; b >= 0; --b) {
-        const bool grouped = seg_grouped(b, p.method[b]);
-        const unsigned int items = grouped ? (p.count[b] + SEG_WARPS - 1) / SEG_WARPS : p.count[b];
+        const unsigned int per = (unsigned int)seg_per_item(b, p.method[b]);
+        const unsigned int items = (p.count[b] + per - 1) / per;
         if (item < base + items) {
             *bin = b;
-            *first = grouped ? (item - base) * SEG_WARPS : item - base;
+            *first = (item - base) * per;
             return;
         }
         base += items;
@@ -110,7 +120,8 @@ static __global__ void k_seg_items(SegPlan* plan, SegMethods methods) {
         unsigned int t = plan->count[SEG_BIN_LARGE] + (plan->count[SEG_BIN_WARP] + SEG_WARPS - 1) / SEG_WARPS;
         for (int b = 0; b < SEG_BLOCK_BINS; ++b) {
             plan->method[b] = methods.m[b];
-            t += seg_grouped(b, methods.m[b]) ? (plan->count[b] + SEG_WARPS - 1) / SEG_WARPS : plan->count[b];
+            const unsigned int per = (unsigned int)seg_per_item(b, methods.m[b]);
+            t += (plan->count[b] + per - 1) / per;
         }
         plan->items = t;
     }
@@ -407,6 +418,46 @@ __device__ __forceinline__ void msd_for_keys(const U* __restrict__ src, int len,
     }
 }
 
+// Sub-ranges d0 .. d0 + per - 1 of a placement whose packed 16-bit counters
+// (wd) now hold each sub-range's end: each sub-range sorted on its own, two
+// or three keys from registers, longer ones by insertion (rare: about one or
+// two keys a sub-range).
+template <typename U>
+__device__ __forceinline__ void msd_finish_subranges(U* sk, const unsigned int* wd, int d0, int per) {
+    auto end_of = [&](int d) { return (int)((wd[d >> 1] >> ((d & 1) * 16)) & 0xffffu); };
+    int r = d0 == 0 ? 0 : end_of(d0 - 1);
+    for (int q = 0; q < per; ++q) {
+        const int e = end_of(d0 + q);
+        const int k = e - r;
+        if (k == 2) {
+            const U a = sk[r], b = sk[r + 1];
+            if (a > b) {
+                sk[r] = b;
+                sk[r + 1] = a;
+            }
+        } else if (k == 3) {
+            U a = sk[r], b = sk[r + 1], c = sk[r + 2];
+            if (a > b) { const U t = a; a = b; b = t; }
+            if (b > c) { const U t = b; b = c; c = t; }
+            if (a > b) { const U t = a; a = b; b = t; }
+            sk[r] = a;
+            sk[r + 1] = b;
+            sk[r + 2] = c;
+        } else if (k > 3) {
+            for (int i = r + 1; i < e; ++i) {
+                const U v = sk[i];
+                int j = i - 1;
+                while (j >= r && sk[j] > v) {
+                    sk[j + 1] = sk[j];
+                    --j;
+                }
+                sk[j + 1] = v;
+            }
+        }
+        r = e;
+    }
+}
+
 template <typename U>
 struct MsdSmem {
     static constexpr size_t misc = MSD_SMEM - 1024;                        // warp totals, reductions, item ids
@@ -539,21 +590,9 @@ __device__ void msd_core(const U* src, U* dst, U* scratch, int len, unsigned cha
         sk[half(atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16)), d)] = k;
     });
     __syncthreads();
-    // pass 4: every owner insertion-sorts its run of sub-ranges
-    if (tid < owners) {
-        const int d0 = tid * per;
-        const int r0 = d0 == 0 ? 0 : (int)half(wd[(d0 - 1) >> 1], d0 - 1);
-        const int r1 = (int)half(wd[(d0 + per - 1) >> 1], d0 + per - 1);
-        for (int i = r0 + 1; i < r1; ++i) {
-            const U v = sk[i];
-            int j = i - 1;
-            while (j >= r0 && sk[j] > v) {
-                sk[j + 1] = sk[j];
-                --j;
-            }
-            sk[j + 1] = v;
-        }
-    }
+    // pass 4: every owner sorts each of its sub-ranges (keys are in order
+    // from one sub-range to the next)
+    if (tid < owners) msd_finish_subranges<U>(sk, wd, tid * per, per);
     __syncthreads();
     for (int i = tid; i < len; i += 1024) dst[i] = from_key<U, XF>(sk[i]);
     __syncthreads();
@@ -698,6 +737,148 @@ __device__ void msd_sort(const U* src, U* dst, U* scratch, int len, unsigned cha
     else msd_core<U, XF>(src, dst, scratch, len, sm);
 }
 
+// ---- several segments a CTA: the MSD routine by thread groups ---------------
+// A group of G threads (its own slice of shared memory and its own named
+// barrier) sorts one segment of up to SegGroup::cap keys as msd_core does:
+// the key range, counts per sub-range (about one key each), placement by
+// sub-range, insertion sorts of each thread's run of sub-ranges. A segment
+// whose keys crowd one sub-range is sorted by a bitonic network in the
+// group's slice instead. The CTA runs SEG_THREADS / G groups side by side.
+template <typename U, int G>
+struct SegGroup {
+    static constexpr int GROUPS = SEG_THREADS / G;
+    static constexpr size_t slice = (size_t)MSD_SMEM / GROUPS / 128 * 128;
+    static constexpr int cap = G == 256 ? 4096 : SegCfg<U>::CAP;    // the bin it serves
+    static constexpr int sub_bits = G == 256 ? 12 : 14;
+    static constexpr size_t key_bytes = (size_t)cap * sizeof(U);
+    static constexpr size_t cnt_off = key_bytes;                     // 16-bit counters, two a word
+    static constexpr size_t misc_off = cnt_off + (size_t)(1 << sub_bits) * 2;
+    static_assert(misc_off + 256 <= slice, "a group's keys, counters and scratch fit its slice");
+};
+
+template <typename U, int XF, int G>
+__device__ void msd_group(const U* src, U* dst, int len, unsigned char* sm, int bar) {
+    using S = SegGroup<U, G>;
+    U* sk = reinterpret_cast<U*>(sm);
+    unsigned int* wd = reinterpret_cast<unsigned int*>(sm + S::cnt_off);
+    int* warp_tot = reinterpret_cast<int*>(sm + S::misc_off);                       // [G / 32]
+    unsigned long long* red = reinterpret_cast<unsigned long long*>(sm + S::misc_off + 128);  // [3]
+    const int tid = threadIdx.x % G, lane = tid & 31, warp = tid >> 5;
+    auto gsync = [&]() { asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(G) : "memory"); };
+    auto half = [](unsigned int w, int d) { return (w >> ((d & 1) * 16)) & 0xffffu; };
+    if (len <= 1) {
+        if (len == 1 && tid == 0) dst[0] = src[0];
+        return;
+    }
+    // the key range (every pass reads the segment again: from L2 after the first)
+    if (tid == 0) {
+        red[0] = ~0ull;
+        red[1] = 0ull;
+        red[2] = 0ull;
+    }
+    gsync();
+    unsigned long long mn = ~0ull, mx = 0ull;
+    for (int i = tid; i < len; i += G) {
+        const unsigned long long k = (unsigned long long)to_key<U, XF>(src[i]);
+        mn = k < mn ? k : mn;
+        mx = k > mx ? k : mx;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long x = __shfl_xor_sync(0xffffffffu, mn, o);
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, mx, o);
+        mn = x < mn ? x : mn;
+        mx = y > mx ? y : mx;
+    }
+    if (lane == 0) {
+        atomicMin(&red[0], mn);
+        atomicMax(&red[1], mx);
+    }
+    gsync();
+    const unsigned long long kmin = red[0], kmax = red[1];
+    if (kmin == kmax) {  // every key equal
+        for (int i = tid; i < len; i += G) dst[i] = src[i];
+        gsync();
+        return;
+    }
+    int bits = 1;
+    while (bits < S::sub_bits && (2 << bits) <= len) ++bits;
+    const int nb = 1 << bits;
+    const int per = nb >= 2 * G ? nb / G : 2;
+    const int owners = nb / per;
+    const float scale = (float)nb / __ull2float_ru(kmax - kmin);
+    auto digit = [&](unsigned long long k) { return min(nb - 1, (int)(__ull2float_rz(k - kmin) * scale)); };
+    for (int w = tid; w < nb / 2; w += G) wd[w] = 0u;
+    gsync();
+    for (int i = tid; i < len; i += G) {
+        const int d = digit((unsigned long long)to_key<U, XF>(src[i]));
+        atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16));
+    }
+    gsync();
+    unsigned int sum = 0, m = 0;
+    if (tid < owners)
+        for (int q = 0; q < per / 2; ++q) {
+            const unsigned int w = wd[tid * (per / 2) + q];
+            sum += (w & 0xffffu) + (w >> 16);
+            m = max(m, max(w & 0xffffu, w >> 16));
+        }
+    unsigned int x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 31) warp_tot[warp] = (int)x;
+    if (lane == 0) atomicMax(reinterpret_cast<unsigned int*>(&red[2]), m);
+    gsync();
+    unsigned int run = x - sum;
+    for (int w = 0; w < warp; ++w) run += (unsigned int)warp_tot[w];
+    if (tid < owners)
+        for (int q = 0; q < per / 2; ++q) {
+            const unsigned int w = wd[tid * (per / 2) + q];
+            const unsigned int s0 = run, s1 = run + (w & 0xffffu);
+            run = s1 + (w >> 16);
+            wd[tid * (per / 2) + q] = s0 | (s1 << 16);
+        }
+    gsync();
+    if (reinterpret_cast<unsigned int*>(&red[2])[0] > (unsigned int)MSD_SUB_MAX) {
+        // crowded: a bitonic network over the slice's keys
+        int p2 = 1;
+        while (p2 < len) p2 <<= 1;
+        for (int i = tid; i < p2; i += G) sk[i] = i < len ? to_key<U, XF>(src[i]) : (U)~(U)0;
+        gsync();
+        for (int k = 2; k <= p2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = tid; i < p2 / 2; i += G) {
+                    const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
+                    const int hi = lo | j;
+                    const bool up = (lo & k) == 0;
+                    const U a = sk[lo], b = sk[hi];
+                    if ((a > b) == up) {
+                        sk[lo] = b;
+                        sk[hi] = a;
+                    }
+                }
+                gsync();
+            }
+        }
+        for (int i = tid; i < len; i += G) dst[i] = from_key<U, XF>(sk[i]);
+        gsync();
+        return;
+    }
+    // place by sub-range; each counter ends at its sub-range's end
+    for (int i = tid; i < len; i += G) {
+        const U k = to_key<U, XF>(src[i]);
+        const int d = digit((unsigned long long)k);
+        sk[half(atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16)), d)] = k;
+    }
+    gsync();
+    // every owner sorts each of its sub-ranges
+    if (tid < owners) msd_finish_subranges<U>(sk, wd, tid * per, per);
+    gsync();
+    for (int i = tid; i < len; i += G) dst[i] = from_key<U, XF>(sk[i]);
+    gsync();
+}
+
 // One slice of up to 4096 keys of 4 or 8 bytes by one CTA: the plain sort's
 // short-slice tier above the warp networks (src/small.rs:11 sorts up to 512
 // with its networks; here the one-pass MSD routine takes 1025..4096 keys, a
@@ -759,6 +940,22 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
                 const unsigned int s = lists[(size_t)SEG_BIN_WARP * n_seg + idx];
                 const unsigned long long b = offsets[s];
                 seg_warp_sort<U, XF>(data_in + b, data + b, (int)(offsets[s + 1] - b), lane);
+            }
+        } else if (methods.m[bin] == SEG_MSD_GROUPS) {
+            if constexpr (sizeof(U) >= 4) {
+                auto run = [&](auto g_tag) {
+                    constexpr int G = decltype(g_tag)::value;
+                    const int g = threadIdx.x / G;
+                    const unsigned int idx = first + (unsigned int)g;
+                    if (idx < plan->count[bin]) {
+                        const unsigned int s = lists[(size_t)bin * n_seg + idx];
+                        const unsigned long long b = offsets[s];
+                        msd_group<U, XF, G>(data_in + b, data + b, (int)(offsets[s + 1] - b),
+                                            smem + (size_t)g * SegGroup<U, G>::slice, 1 + g);
+                    }
+                };
+                if (bin == 2) run(std::integral_constant<int, 256>{});
+                else run(std::integral_constant<int, 512>{});
             }
         } else if (seg_grouped(bin, methods.m[bin])) {
             const unsigned int idx = first + warp;
