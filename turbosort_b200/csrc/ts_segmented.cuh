@@ -418,43 +418,25 @@ __device__ __forceinline__ void msd_for_keys(const U* __restrict__ src, int len,
     }
 }
 
-// Sub-ranges d0 .. d0 + per - 1 of a placement whose packed 16-bit counters
-// (wd) now hold each sub-range's end: each sub-range sorted on its own, two
-// or three keys from registers, longer ones by insertion (rare: about one or
-// two keys a sub-range).
+// The run of sub-ranges d0 .. d0 + per - 1 of a placement whose packed
+// 16-bit counters (wd) now hold each sub-range's end, insertion-sorted as
+// one run: keys are in order from one sub-range to the next, so only keys
+// inside a sub-range (about one or two) move. (Sorting each sub-range on its
+// own, two or three keys from registers, measured slower: 2.90 against 2.50
+// ms for 10,485 segments of 30,000 keys.)
 template <typename U>
-__device__ __forceinline__ void msd_finish_subranges(U* sk, const unsigned int* wd, int d0, int per) {
+__device__ __forceinline__ void msd_insert_run(U* sk, const unsigned int* wd, int d0, int per) {
     auto end_of = [&](int d) { return (int)((wd[d >> 1] >> ((d & 1) * 16)) & 0xffffu); };
-    int r = d0 == 0 ? 0 : end_of(d0 - 1);
-    for (int q = 0; q < per; ++q) {
-        const int e = end_of(d0 + q);
-        const int k = e - r;
-        if (k == 2) {
-            const U a = sk[r], b = sk[r + 1];
-            if (a > b) {
-                sk[r] = b;
-                sk[r + 1] = a;
-            }
-        } else if (k == 3) {
-            U a = sk[r], b = sk[r + 1], c = sk[r + 2];
-            if (a > b) { const U t = a; a = b; b = t; }
-            if (b > c) { const U t = b; b = c; c = t; }
-            if (a > b) { const U t = a; a = b; b = t; }
-            sk[r] = a;
-            sk[r + 1] = b;
-            sk[r + 2] = c;
-        } else if (k > 3) {
-            for (int i = r + 1; i < e; ++i) {
-                const U v = sk[i];
-                int j = i - 1;
-                while (j >= r && sk[j] > v) {
-                    sk[j + 1] = sk[j];
-                    --j;
-                }
-                sk[j + 1] = v;
-            }
+    const int r0 = d0 == 0 ? 0 : end_of(d0 - 1);
+    const int r1 = end_of(d0 + per - 1);
+    for (int i = r0 + 1; i < r1; ++i) {
+        const U v = sk[i];
+        int j = i - 1;
+        while (j >= r0 && sk[j] > v) {
+            sk[j + 1] = sk[j];
+            --j;
         }
-        r = e;
+        sk[j + 1] = v;
     }
 }
 
@@ -590,9 +572,9 @@ __device__ void msd_core(const U* src, U* dst, U* scratch, int len, unsigned cha
         sk[half(atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16)), d)] = k;
     });
     __syncthreads();
-    // pass 4: every owner sorts each of its sub-ranges (keys are in order
-    // from one sub-range to the next)
-    if (tid < owners) msd_finish_subranges<U>(sk, wd, tid * per, per);
+    // pass 4: every owner insertion-sorts its run of sub-ranges (out of order
+    // only inside sub-ranges, of about one or two keys)
+    if (tid < owners) msd_insert_run<U>(sk, wd, tid * per, per);
     __syncthreads();
     for (int i = tid; i < len; i += 1024) dst[i] = from_key<U, XF>(sk[i]);
     __syncthreads();
@@ -872,8 +854,8 @@ __device__ void msd_group(const U* src, U* dst, int len, unsigned char* sm, int 
         sk[half(atomicAdd(&wd[d >> 1], 1u << ((d & 1) * 16)), d)] = k;
     }
     gsync();
-    // every owner sorts each of its sub-ranges
-    if (tid < owners) msd_finish_subranges<U>(sk, wd, tid * per, per);
+    // every owner insertion-sorts its run of sub-ranges
+    if (tid < owners) msd_insert_run<U>(sk, wd, tid * per, per);
     gsync();
     for (int i = tid; i < len; i += G) dst[i] = from_key<U, XF>(sk[i]);
     gsync();
@@ -941,7 +923,7 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
                 const unsigned long long b = offsets[s];
                 seg_warp_sort<U, XF>(data_in + b, data + b, (int)(offsets[s + 1] - b), lane);
             }
-        } else if (methods.m[bin] == SEG_MSD_GROUPS) {
+        } else if (bin < SEG_BLOCK_BINS && methods.m[bin] == SEG_MSD_GROUPS) {
             if constexpr (sizeof(U) >= 4) {
                 auto run = [&](auto g_tag) {
                     constexpr int G = decltype(g_tag)::value;
@@ -957,7 +939,7 @@ __global__ void __launch_bounds__(SEG_THREADS, 1)
                 if (bin == 2) run(std::integral_constant<int, 256>{});
                 else run(std::integral_constant<int, 512>{});
             }
-        } else if (seg_grouped(bin, methods.m[bin])) {
+        } else if (bin < SEG_BLOCK_BINS && seg_grouped(bin, methods.m[bin])) {
             const unsigned int idx = first + warp;
             if (idx < plan->count[bin]) {
                 const unsigned int s = lists[(size_t)bin * n_seg + idx];
