@@ -97,6 +97,7 @@ unsigned long long ts_ctx_launches(const ts_ctx *ctx);
 typedef struct ts_sort_info {
     int32_t tier, mode, passes, divert_shift;
     int32_t pass_digit[16];
+    int32_t digit_bits;  /* the LSD's digit width; pass_digit[i] * digit_bits is a pass's shift */
 } ts_sort_info;
 ts_status ts_ctx_last_sort_info(ts_ctx *ctx, ts_sort_info *info);
 
@@ -197,16 +198,22 @@ ts_status ts_segments_methods(ts_ctx *ctx, size_t key_bytes, int *methods, int s
  * and thresholds are compile-time constants measured on its author's CPUs,
  * src/radix/mod.rs:38-54). Each onesweep tile variant (keys a thread: 22, 11,
  * 5 for 4-byte keys; 11, 5, 2 for 8-byte; 32, 16, 8 for 2-byte; 8-bit digits)
- * is timed on random keys of one length per length bin (n < 2^22, n < 2^25,
- * larger) and the fastest is kept per key width and bin; ms, if not null,
- * receives the 3 x 3 median times (bin-major). ts_lsd_variants reads (set = 0)
- * or sets (set = 1) the three variants of a key width; ts_lsd_variant_ipt
- * gives a variant's keys a thread. */
+ * and the 9-, 10- and 11-bit digit widths are timed on random keys of one
+ * length per length bin (n < 2^22, n < 2^25, larger) and the fastest is kept
+ * per key width and bin; ms, if not null, receives the 3 x 6 median times
+ * (bin-major: the three 8-bit variants, then 9, 10 and 11 bits).
+ * ts_lsd_variants reads (set = 0) or sets (set = 1) the three variants of a
+ * key width; ts_lsd_variant_ipt gives a variant's keys a thread.
+ * ts_lsd_digit_bits reads or sets the digit width per length bin, 4..11 bits
+ * (the crate sorts with 8-bit digits and, for long u64 slices, 11-bit ones,
+ * src/radix/mod.rs:43-54); widths other than 8 apply to keys-only sorts of
+ * fewer than 2^31 keys and never divert. */
 ts_status ts_lsd_autotune(ts_ctx *ctx, size_t key_bytes, float *ms);
 ts_status ts_lsd_variants(ts_ctx *ctx, size_t key_bytes, int *variants, int set);
 int ts_lsd_variant_ipt(size_t key_bytes, int variant);
-/* The tuning cache: the LSD variants and the segmented sort's methods of every
- * key width, in a JSON file keyed by the GPU's name. _load leaves the context
+ts_status ts_lsd_digit_bits(ts_ctx *ctx, size_t key_bytes, int *bits, int set);
+/* The tuning cache: the LSD variants and digit widths and the segmented
+ * sort's methods of every key width, in a JSON file keyed by the GPU's name. _load leaves the context
  * as it is when the file is missing or was written on another GPU, and sets
  * *loaded to 1 when it took the file's choices. */
 ts_status ts_ctx_tune_save(ts_ctx *ctx, const char *path);

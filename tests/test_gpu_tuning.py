@@ -2,9 +2,11 @@
 
 Every variant the tuner can pick sorts exactly like the oracle, for each key
 width it tunes (2, 4 and 8 bytes; unsigned, signed and float transforms), at
-lengths in each of its three length bins; the tuner's choice per bin is one
-of its variants, and the tuning cache round-trips through its JSON file and
-is ignored when it was written on another GPU."""
+lengths in each of its three length bins; the tuner's choice per bin is the
+fastest of its candidates (8-bit tile variants, 9-11-bit digits), and the
+tuning cache round-trips through its JSON file, takes 8-bit digits from a file
+without widths, rejects a width outside 4..11, and is ignored when it was
+written on another GPU. Every digit width's parity is in test_gpu_digit_bits.py."""
 import json
 
 import numpy as np
@@ -69,16 +71,29 @@ def test_autotune_and_cache(env, tmp_path):
     torch, ts, O, ctx = env
     r = ctx.lsd_autotune(4)
     assert len(r["variants"]) == 3 and all(v in (0, 1, 2) for v in r["variants"])
-    assert all(ms > 0 for row in r["ms"] for ms in row)
-    for b, v in enumerate(r["variants"]):  # the choice is the fastest measured
-        assert r["ms"][b][v] == min(r["ms"][b])
+    assert all(b in (8, 9, 10, 11) for b in r["digit_bits"])
+    assert all(ms > 0 for row in r["ms"] for ms in row) and all(len(row) == 6 for row in r["ms"])
+    for b, (v, bits) in enumerate(zip(r["variants"], r["digit_bits"])):  # the choice is the fastest measured
+        assert r["ms"][b][v if bits == 8 else 3 + bits - 9] == min(r["ms"][b])
     path = str(tmp_path / "tune.json")
     ctx.tune_save(path)
     doc = json.load(open(path))
-    assert doc["lsd"]["4"] == r["variants"]
+    assert doc["lsd"]["4"] == r["variants"] and doc["lsd_bits"]["4"] == r["digit_bits"]
     other = ts.Context(0)
     other.lsd_variants(4, [2, 2, 2])
+    other.lsd_digit_bits(4, [5, 5, 5])
     assert other.tune_load(path) and other.lsd_variants(4) == r["variants"]
+    assert other.lsd_digit_bits(4) == r["digit_bits"]
+    # a file written before digit widths were tuned loads with 8-bit digits
+    del doc["lsd_bits"]
+    json.dump(doc, open(path, "w"))
+    other.lsd_digit_bits(4, [5, 5, 5])
+    assert other.tune_load(path) and other.lsd_digit_bits(4) == [8, 8, 8]
+    doc["lsd_bits"] = {"2": [8, 8, 8], "4": [8, 12, 8], "8": [8, 8, 8]}
+    json.dump(doc, open(path, "w"))
+    with pytest.raises(ts.TurbosortError):
+        other.tune_load(path)
+    del doc["lsd_bits"]
     doc["gpu"] = "some other GPU"
     json.dump(doc, open(path, "w"))
     other.lsd_variants(4, [2, 2, 2])

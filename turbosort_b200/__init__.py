@@ -83,11 +83,11 @@ class LearnedStats(ctypes.Structure):
 class SortInfo(ctypes.Structure):
     """ts_sort_info: what the context's last plain sort did."""
     _fields_ = [("tier", ctypes.c_int32), ("mode", ctypes.c_int32), ("passes", ctypes.c_int32),
-                ("divert_shift", ctypes.c_int32), ("pass_digit", ctypes.c_int32 * 16)]
+                ("divert_shift", ctypes.c_int32), ("pass_digit", ctypes.c_int32 * 16), ("digit_bits", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {"tier": self.tier, "mode": self.mode, "passes": self.passes, "divert_shift": self.divert_shift,
-                "pass_digit": list(self.pass_digit[:self.passes])}
+                "pass_digit": list(self.pass_digit[:self.passes]), "digit_bits": self.digit_bits}
 
 
 def lsd_variant_ipt(key_bytes: int, variant: int) -> int:
@@ -181,6 +181,8 @@ def lib() -> ctypes.CDLL:
             L.ts_lsd_variants.restype = st
             L.ts_lsd_variant_ipt.argtypes = [sz, i]
             L.ts_lsd_variant_ipt.restype = i
+            L.ts_lsd_digit_bits.argtypes = [vp, sz, ctypes.POINTER(ctypes.c_int), i]
+            L.ts_lsd_digit_bits.restype = st
             L.ts_ctx_tune_save.argtypes = [vp, ctypes.c_char_p]
             L.ts_ctx_tune_save.restype = st
             L.ts_ctx_tune_load.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
@@ -259,14 +261,25 @@ class Context:
         self._check(lib().ts_ctx_transfer_pipeline(self._h, chunks, min_bytes))
 
     def lsd_autotune(self, key_bytes: int) -> dict:
-        """Time every onesweep tile variant per length bin for keys of this
-        width and keep the fastest; returns the choices and the times."""
-        ms = (ctypes.c_float * 9)()
+        """Time every 8-bit onesweep tile variant and the 9-, 10- and 11-bit
+        digit widths per length bin for keys of this width and keep the
+        fastest; returns the choices and the times (per bin: the three 8-bit
+        variants, then 9, 10 and 11 bits)."""
+        ms = (ctypes.c_float * 18)()
         self._check(lib().ts_lsd_autotune(self._h, key_bytes, ms))
         v = self.lsd_variants(key_bytes)
         return {"variants": v, "keys_per_thread": [lsd_variant_ipt(key_bytes, x) for x in v],
-                "ms": [[round(ms[b * 3 + x], 4) for x in range(3)] for b in range(3)],
+                "digit_bits": self.lsd_digit_bits(key_bytes),
+                "ms": [[round(ms[b * 6 + x], 4) for x in range(6)] for b in range(3)],
                 "bins": ["n < 2^22", "n < 2^25", "larger"]}
+
+    def lsd_digit_bits(self, key_bytes: int, bits=None) -> list[int]:
+        """The plain LSD's digit width (4..11) per length bin for this key
+        width (set when given; widths other than 8 apply to keys-only sorts
+        below 2^31 keys)."""
+        arr = (ctypes.c_int * 3)(*(bits or [8, 8, 8]))
+        self._check(lib().ts_lsd_digit_bits(self._h, key_bytes, arr, int(bits is not None)))
+        return list(arr)
 
     def lsd_variants(self, key_bytes: int, variants=None) -> list[int]:
         """The tile variant per length bin for this key width (set when given)."""

@@ -421,6 +421,7 @@ ts_status ts_ctx_last_sort_info(ts_ctx* c, ts_sort_info* info) {
     info->passes = p.n_live;
     info->divert_shift = p.divert_shift;
     for (int i = 0; i < p.n_live && i < 16; ++i) info->pass_digit[i] = p.pass[i];
+    info->digit_bits = c->last_bits;
     return TS_OK;
 }
 

@@ -48,6 +48,8 @@ struct ts_ctx {
     // per key width (1, 2, 4, 8 bytes) and length bin (< 2^22, < 2^25, more),
     // set by ts_lsd_autotune; the defaults were measured on a B200
     int lsd_variant[4][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 0}, {0, 0, 0}};
+    // the plain LSD's digit width per key width and length bin (4..11 bits)
+    int lsd_bits[4][3] = {{8, 8, 8}, {8, 8, 8}, {8, 8, 8}, {8, 8, 8}};
     // segmented sort: the method of each on-chip length bin per key width
     // (1, 2, 4, 8 bytes), set by the autotuner; and the last captured graph
     int seg_methods[4][4] = {{4, 5, 2, 2}, {4, 5, 2, 2}, {4, 5, 6, 6}, {4, 3, 6, 6}};
@@ -82,6 +84,7 @@ struct ts_ctx {
     uint32_t test_spin_limit = 0;
     // the tier of the last plain sort (ts_sort_info: 1 small, 2 counting, 3 LSD)
     int last_tier = 0;
+    int last_bits = 8;  // the last LSD sort's digit width
 
     std::string last_error;
     unsigned long long launches = 0;   // kernels this context has launched

@@ -33,9 +33,18 @@ constexpr int LSD_VARIANTS = 3;
 constexpr int LSD_BINS = 3;  // n < 2^22, n < 2^25, larger
 static inline int lsd_bin(size_t n) { return n < ((size_t)1 << 22) ? 0 : n < ((size_t)1 << 25) ? 1 : 2; }
 
-template <typename U, bool PAIRS, int V = 0>
+// Digit widths of the plain LSD: 8 bits by default (the crate's byte core,
+// src/radix/mod.rs:205-271); keys-only sorts below 2^31 keys can also run
+// 4..11-bit digits (the crate's wide core takes 11, src/radix/mod.rs:43-54,
+// 518-600), chosen per key width and length bin (ts_lsd_digit_bits, or the
+// autotuner).
+constexpr int LSD_MIN_BITS = 4;
+constexpr int LSD_MAX_BITS = 11;
+
+template <typename U, bool PAIRS, int V = 0, int B = 8>
 struct LsdCfg {
-    static constexpr int BITS = 8;
+    static constexpr int BITS = B;
+    static_assert(B >= LSD_MIN_BITS && B <= LSD_MAX_BITS && (B == 8 || (!PAIRS && V == 0)), "digit width");
     static constexpr int THREADS = 512;
     // the first live pass of a keys-only sort ranks with shared atomics
     // (k_onesweep, UNSTABLE1)
@@ -49,18 +58,32 @@ struct LsdCfg {
     // two threads walk each digit's look-back (k_onesweep LB_PAIR): 2^27 u64
     // keys without diverting 6.62 -> 6.47 ms; 2^28 u32 keys 4.22 -> 4.38 ms,
     // so 8-byte keys only
-    static constexpr bool LB_PAIR = sizeof(U) == 8 && !PAIRS;
+    static constexpr bool LB_PAIR = sizeof(U) == 8 && !PAIRS && B == 8;
     // 8-byte keys without positions divert (src/radix/divert.rs): the plan may
     // leave out the lowest live digits, and k_divert_runs / k_divert_long
     // finish the runs that leaves
-    static constexpr bool DIVERT = !PAIRS && sizeof(U) == 8;
+    static constexpr bool DIVERT = !PAIRS && sizeof(U) == 8 && B == 8;
+    // 64-bit offsets (more than 2^31 keys) are compiled for 8-bit digits only
+    static constexpr bool HUGE_OK = B == 8;
     // the largest tile for which two CTAs (one tile of keys and positions, the
     // staging tile, 32-bit per-warp counters) share one SM's shared memory:
     // the per-tile costs (look-back, counter scans) shrink per key as tiles
     // grow, which on a B200 outweighs double-buffering a smaller tile
     // (2^28 u32 keys: 15 keys a thread double-buffered 5.18 ms, 22 single 4.83 ms)
     static constexpr int IPT0 = sizeof(U) == 8 ? (PAIRS ? 7 : 11) : (PAIRS ? 11 : (sizeof(U) == 4 ? 22 : 32));
-    static constexpr int IPT = IPT0 >> V;
+    // Other digit widths (keys only): per-warp counters take 16 x 2^B words,
+    // so wider digits leave less room for the tile. The largest tile (up to
+    // IPT0 keys a thread) with which two CTAs still share an SM, if that
+    // leaves at least 8 keys a thread; else the largest for one CTA an SM.
+    static constexpr int fit_ipt(size_t budget) {
+        const size_t fixed = (size_t)16 * (1u << B) * 4 + (size_t)(1u << B) * 8 + 1024;
+        return budget > fixed ? (int)((budget - fixed) / (2 * sizeof(U) * THREADS)) : 0;
+    }
+    static constexpr int ipt_for_bits() {
+        return fit_ipt(113 * 1024) >= 8 ? (fit_ipt(113 * 1024) < IPT0 ? fit_ipt(113 * 1024) : IPT0)
+                                        : (fit_ipt(226 * 1024) < IPT0 ? fit_ipt(226 * 1024) : IPT0);
+    }
+    static constexpr int IPT = B == 8 ? IPT0 >> V : ipt_for_bits();
     static_assert(V >= 0 && V < LSD_VARIANTS && IPT >= 1, "tile variant");
     static constexpr int NBUF = 1;  // tiles of keys in flight per CTA; the next one is prefetched into L2
     // items with i % MATCH_MOD < MATCH_CNT find their digit's peers with
@@ -72,7 +95,8 @@ struct LsdCfg {
     // in three 6.71)
     static constexpr int MATCH_MOD = (sizeof(U) == 8 || PAIRS) ? 4 : 3;
     static constexpr int MATCH_CNT = 1;
-    using Smem = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
+    using Smem = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF, LB_PAIR>;
+    static_assert(Smem::bytes <= 227 * 1024, "one CTA's shared memory");
     static constexpr int TILE = Smem::TILE;
     static constexpr int RADIX = 1 << BITS;
     static constexpr int ND = (Bits<U>::W + BITS - 1) / BITS;
@@ -87,7 +111,7 @@ struct MetaLayout {
         m.scan_off = o;
         o += 256;
         m.plan_off = o;
-        o += 256;
+        o += 512;
         m.counters_off = o;
         o += ((size_t)launches * 4 + 255) / 256 * 256;
         m.hist_off = o;
@@ -178,7 +202,7 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     {
         constexpr int T = 1024;
         const size_t smem = (size_t)ND * RADIX * hist_copies<RADIX, ND>() * 4;
-        static_assert(144 + 8 * ND <= 256, "the plan area holds every digit's largest bucket");
+        static_assert(144 + 8 * ND <= 512, "the plan area holds every digit's largest bucket");
         auto kern = k_hist<U, XF, C::BITS, T, C::DIVERT>;
         const int occ = occupancy(c, kern, T, smem);
         TS_CUDA(c, launch_dep(c, kern, c->sm_count * occ, T, smem, in, n, st, hist, vec_ok, bins, plan, PAIRS ? 1 : 0,
@@ -187,11 +211,15 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     }
     {
         using Sm = typename C::Smem;
-        auto kern = n <= (size_t)0x7fffffff
-                        ? k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>
-                        : k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD,
-                                     C::MATCH_CNT, C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>;
+        auto kern = k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD, C::MATCH_CNT,
+                               C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>;
+        if constexpr (C::HUGE_OK) {
+            if (n > (size_t)0x7fffffff)
+                kern = k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD, C::MATCH_CNT,
+                                  C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>;
+        } else {
+            if (n > (size_t)0x7fffffff) return fail(c, TS_ERR_INTERNAL, "digit width without 64-bit offsets");
+        }
         const int occ = occupancy(c, kern, C::THREADS, Sm::bytes);
         SweepArgs<U, PAIRS> a{};
         a.in = in;
@@ -230,6 +258,13 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     *plan_out = plan;
     return TS_OK;
 }
+
+// The LSD passes of a keys-only sort of n <= 2^31 - 1 keys at a digit width
+// of LSD_MIN_BITS..LSD_MAX_BITS other than 8 (sorted keys end in d_data or,
+// after an odd pass count, d_alt, as the plan says). Compiled apart from the
+// 8-bit sorts, in ts_width_*.cu.
+template <typename U, int XF>
+ts_status run_lsd_bits(ts_ctx* c, int bits, U* d_data, U* d_alt, size_t n, Plan** plan);
 
 template <typename U, int XF>
 ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
@@ -297,10 +332,15 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
             occupancy_of((const void*)k_divert_long<U, XF>, SEG_THREADS, MSD_SMEM);
         }
         const int variant = c->lsd_variant[width_slot(sizeof(U))][lsd_bin(n)];
+        // a digit width other than 8 (keys below 2^31 only); it never diverts
+        const int bits = n <= (size_t)0x7fffffff ? c->lsd_bits[width_slot(sizeof(U))][lsd_bin(n)] : 8;
+        c->last_bits = bits;
         auto enqueue = [&]() -> ts_status {
             Plan* plan = nullptr;
             ts_status st;
-            if (variant == 1)
+            if (bits != 8)
+                st = run_lsd_bits<U, XF>(c, bits, d_data, d_alt, n, &plan);
+            else if (variant == 1)
                 st = run_lsd<U, XF, false, LsdCfg<U, false, 1>>(c, d_data, d_alt, d_data, nullptr, nullptr, nullptr, n,
                                                                 1, &plan);
             else if (variant == 2)
@@ -315,16 +355,18 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
                                   (int)(aligned16(d_alt) && aligned16(d_data))));
             ++c->launches;
             if constexpr (DIVERT) {
-                const MetaLayout m = MetaLayout::make(LsdCfg<U, false>::ND, LsdCfg<U, false>::RADIX, 0);
-                char* dv = (char*)c->meta.p + m.divert_off();
-                unsigned long long* n_runs = (unsigned long long*)dv;
-                unsigned int* counter = (unsigned int*)(dv + 8);
-                mark(c, "divert");
-                k_divert_runs<U, XF><<<c->sm_count * 8, 256, 0, c->stream>>>(
-                    plan, d_data, n, (unsigned long long*)c->runs.p, n_runs, runs_cap, c->d_error, aligned16(d_data));
-                k_divert_long<U, XF><<<c->sm_count, SEG_THREADS, MSD_SMEM, c->stream>>>(
-                    plan, d_data, d_alt, n, (const unsigned long long*)c->runs.p, n_runs, counter, c->d_error);
-                c->launches += 2;
+                if (bits == 8) {
+                    const MetaLayout m = MetaLayout::make(LsdCfg<U, false>::ND, LsdCfg<U, false>::RADIX, 0);
+                    char* dv = (char*)c->meta.p + m.divert_off();
+                    unsigned long long* n_runs = (unsigned long long*)dv;
+                    unsigned int* counter = (unsigned int*)(dv + 8);
+                    mark(c, "divert");
+                    k_divert_runs<U, XF><<<c->sm_count * 8, 256, 0, c->stream>>>(
+                        plan, d_data, n, (unsigned long long*)c->runs.p, n_runs, runs_cap, c->d_error, aligned16(d_data));
+                    k_divert_long<U, XF><<<c->sm_count, SEG_THREADS, MSD_SMEM, c->stream>>>(
+                        plan, d_data, d_alt, n, (const unsigned long long*)c->runs.p, n_runs, counter, c->d_error);
+                    c->launches += 2;
+                }
             }
             mark(c, "end");
             return TS_OK;
@@ -337,7 +379,8 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         if (c->stream) cudaStreamIsCapturing(c->stream, &cs);
         if (!c->use_graphs || !c->stream || c->timing || c->test_spin_limit || cs != cudaStreamCaptureStatusNone)
             return enqueue();
-        const size_t key[9] = {sizeof(U) * 128 + (size_t)XF * 16 + (size_t)variant * 2 + (c->divert ? 1 : 0),
+        const size_t key[9] = {sizeof(U) | (size_t)XF << 4 | (size_t)variant << 8 | (size_t)(c->divert ? 1 : 0) << 12 |
+                                   (size_t)bits << 16,
                                (size_t)d_data, (size_t)d_alt, n,
                                (size_t)c->meta.p, (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p,
                                (size_t)c->runs.p};

@@ -54,7 +54,9 @@ struct SweepArgs {
     int withhold_tile0;          // test hook: tile 0 never publishes (its successors' waits run out)
 };
 
-template <typename U, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF>
+// LBC: the region of each digit's tile count and start that the paired
+// look-back (LB_PAIR) reads; left out otherwise.
+template <typename U, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool LBC>
 struct SweepSmem {
     static constexpr int RADIX = 1 << BITS;
     static constexpr int WARPS = THREADS / 32;
@@ -68,7 +70,7 @@ struct SweepSmem {
     static constexpr size_t cnt_off = al(sv_off + (PAIRS ? (size_t)TILE * 4 : 0));    // [RANK_WARPS][RADIX] u32
     static constexpr size_t gbase_off = al(cnt_off + (size_t)RANK_WARPS * RADIX * 4);  // [RADIX] i64
     static constexpr size_t lbc_off = al(gbase_off + (size_t)RADIX * 8);              // [RADIX] u32 x2: counts, starts
-    static constexpr size_t bar_off = al(lbc_off + (size_t)RADIX * 8);                // [2] mbarrier
+    static constexpr size_t bar_off = al(lbc_off + (LBC ? (size_t)RADIX * 8 : 0));     // [2] mbarrier
     static constexpr size_t misc_off = bar_off + 16;                                  // ints
     static constexpr size_t bytes = misc_off + 4 * 64;
     static_assert(TILE * sizeof(U) % 16 == 0, "bulk copies move multiples of 16 bytes");
@@ -79,35 +81,67 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 // The lanes of a warp whose BITS-bit digit equals this lane's. One ballot per
-// digit bit gives the warp's bit-planes; lane L then builds the entry of two
-// small tables for the digit values it stands for (its low 5 bits, and its
-// low 3 bits for the top digit bits), and each lane reads the two entries of
-// its own digit with a shuffle. xl[b] / xh[b] hold, per lane, all ones where
-// the lane's index has bit b clear (set up once by peer_masks_init).
+// digit bit gives the warp's bit-planes; the digit's bits are taken in
+// groups of up to five, and for each group lane L builds the entry of a
+// small table for the group value L stands for (the lanes whose bits in the
+// group equal L's index); each lane then reads its own digit's entry of every
+// table with a shuffle and ANDs them. x[b] holds, per lane, all ones where
+// the lane's index has bit (b mod 5) clear (set up once by init). 8-bit
+// digits take two tables (5 + 3 bits), 11-bit ones three (5 + 5 + 1).
 template <int BITS>
 struct PeerMasks {
-    static_assert(BITS >= 1 && BITS <= 10, "two lookup tables cover digits of up to 10 bits");
-    static constexpr int LO = BITS < 5 ? BITS : 5;
-    static constexpr int HI = BITS - LO;
-    uint32_t xl[LO];
-    uint32_t xh[HI > 0 ? HI : 1];
+    static_assert(BITS >= 1 && BITS <= 15, "three lookup tables cover digits of up to 15 bits");
+    static constexpr int NT = (BITS + 4) / 5;  // tables
+    uint32_t x[BITS];
     __device__ __forceinline__ void init(int lane) {
 #pragma unroll
-        for (int b = 0; b < LO; ++b) xl[b] = ((lane >> b) & 1) ? 0u : 0xffffffffu;
-#pragma unroll
-        for (int b = 0; b < HI; ++b) xh[b] = ((lane >> b) & 1) ? 0u : 0xffffffffu;
+        for (int b = 0; b < BITS; ++b) x[b] = ((lane >> (b % 5)) & 1) ? 0u : 0xffffffffu;
     }
     __device__ __forceinline__ uint32_t peers(uint32_t d) const {
-        uint32_t lo = 0xffffffffu, hi = 0xffffffffu;
+        uint32_t tbl[NT];
 #pragma unroll
-        for (int b = 0; b < LO; ++b) lo &= __ballot_sync(0xffffffffu, (d >> b) & 1u) ^ xl[b];
+        for (int t = 0; t < NT; ++t) tbl[t] = 0xffffffffu;
 #pragma unroll
-        for (int b = 0; b < HI; ++b) hi &= __ballot_sync(0xffffffffu, (d >> (LO + b)) & 1u) ^ xh[b];
-        uint32_t p = __shfl_sync(0xffffffffu, lo, (int)(d & ((1u << LO) - 1)));
-        if constexpr (HI > 0) p &= __shfl_sync(0xffffffffu, hi, (int)(d >> LO));
+        for (int b = 0; b < BITS; ++b) tbl[b / 5] &= __ballot_sync(0xffffffffu, (d >> b) & 1u) ^ x[b];
+        uint32_t p = 0xffffffffu;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const int w = BITS - 5 * t < 5 ? BITS - 5 * t : 5;
+            p &= __shfl_sync(0xffffffffu, tbl[t], (int)((d >> (5 * t)) & ((1u << w) - 1)));
+        }
         return p;
     }
 };
+
+// D consecutive per-warp counters of one owner thread, moved as one word
+// (D = 1, 2 or 4; the address is D-word aligned).
+template <int D>
+__device__ __forceinline__ void cnt_load(const uint32_t* p, uint32_t (&v)[D]) {
+    static_assert(D == 1 || D == 2 || D == 4, "digits per owner");
+    if constexpr (D == 4) {
+        const uint4 x = *reinterpret_cast<const uint4*>(p);
+        v[0] = x.x, v[1] = x.y, v[2] = x.z, v[3] = x.w;
+    } else if constexpr (D == 2) {
+        const uint2 x = *reinterpret_cast<const uint2*>(p);
+        v[0] = x.x, v[1] = x.y;
+    } else {
+        v[0] = *p;
+    }
+}
+template <int D>
+__device__ __forceinline__ void cnt_store(uint32_t* p, const uint32_t (&v)[D]) {
+    if constexpr (D == 4) *reinterpret_cast<uint4*>(p) = make_uint4(v[0], v[1], v[2], v[3]);
+    else if constexpr (D == 2) *reinterpret_cast<uint2*>(p) = make_uint2(v[0], v[1]);
+    else *p = v[0];
+}
+// WORDS counters (a multiple of 4, 16-byte aligned) set to zero, 16 bytes a store
+template <int WORDS, int THREADS>
+__device__ __forceinline__ void zero_counters(uint32_t* cnt, int tid) {
+    static_assert(WORDS % 4 == 0, "whole 16-byte words");
+    uint4* z = reinterpret_cast<uint4*>(cnt);
+#pragma unroll
+    for (int i = tid; i < WORDS / 4; i += THREADS) z[i] = make_uint4(0u, 0u, 0u, 0u);
+}
 
 // Items i with i % MATCH_MOD < MATCH_CNT find their equal digits with the
 // match.any instruction, which runs on a different pipe from the ballots; the
@@ -121,10 +155,12 @@ struct PeerMasks {
 // observable. With positions (PAIRS) every pass stays stable.
 template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
           int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false, int LBW = LB_WINDOW, bool LB_PAIR = false>
-__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<U, PAIRS> a) {
+__global__ void __launch_bounds__(THREADS, SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF, LB_PAIR>::bytes <= 113 * 1024
+                                               ? 1024 / THREADS
+                                               : 1) k_onesweep(SweepArgs<U, PAIRS> a) {
     dep_wait();
     dep_release();
-    using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF>;
+    using L = SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF, LB_PAIR>;
     using OFF = typename std::conditional<BIG, long long, int>::type;
     constexpr int RADIX = L::RADIX;
     constexpr int TILE = L::TILE;
@@ -175,7 +211,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
         for (size_t i = (size_t)blockIdx.x * THREADS + tid; i < nz; i += (size_t)gridDim.x * THREADS)
             z[i] = make_uint4(0u, 0u, 0u, 0u);
     }
-    for (int i = tid; i < RANK_WARPS * RADIX; i += THREADS) cnt[i] = 0;
+    zero_counters<RANK_WARPS * RADIX, THREADS>(cnt, tid);
     if (tid == 0) {
         for (int b = 0; b < NBUF; ++b) mbar_init(&bars[b], 1);
         fence_mbar_init();
@@ -273,23 +309,26 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
         __syncthreads();
 
         // digit owners: prefix over warps, publish the tile's counts, tile-local starts
+        // (an owner of DPT digits moves their counters as one 8- or 16-byte word)
         uint32_t tcount[DPT];
         uint32_t own = 0;
         if (tid < OWNERS) {
 #pragma unroll
-            for (int q = 0; q < DPT; ++q) {
-                const int r = tid * DPT + q;
-                uint32_t s = 0;
+            for (int q = 0; q < DPT; ++q) tcount[q] = 0;
 #pragma unroll
-                for (int w = 0; w < RANK_WARPS; ++w) {
-                    const uint32_t c = cnt[w * RADIX + r];
-                    cnt[w * RADIX + r] = s;
-                    s += c;
-                }
-                tcount[q] = s;
-                own += s;
+            for (int w = 0; w < RANK_WARPS; ++w) {
+                uint32_t c[DPT];
+                cnt_load<DPT>(cnt + w * RADIX + tid * DPT, c);
+                cnt_store<DPT>(cnt + w * RADIX + tid * DPT, tcount);
+#pragma unroll
+                for (int q = 0; q < DPT; ++q) tcount[q] += c[q];
+            }
+#pragma unroll
+            for (int q = 0; q < DPT; ++q) {
+                own += tcount[q];
                 if (t != 0 || !a.withhold_tile0)
-                    st_relaxed_gpu(a.lookback + (size_t)t * RADIX + r, (t == 0 ? LB_FLAG_INC : LB_FLAG_AGG) | s);
+                    st_relaxed_gpu(a.lookback + (size_t)t * RADIX + tid * DPT + q,
+                                   (t == 0 ? LB_FLAG_INC : LB_FLAG_AGG) | tcount[q]);
             }
         }
         uint32_t x = own;
@@ -312,9 +351,15 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
                     lb_cnt[r] = tcount[q];
                     lb_start[r] = run;
                 }
-#pragma unroll
-                for (int w = 0; w < RANK_WARPS; ++w) cnt[w * RADIX + r] += run;
                 run += tcount[q];
+            }
+#pragma unroll
+            for (int w = 0; w < RANK_WARPS; ++w) {
+                uint32_t c[DPT];
+                cnt_load<DPT>(cnt + w * RADIX + tid * DPT, c);
+#pragma unroll
+                for (int q = 0; q < DPT; ++q) c[q] += lstart[q];
+                cnt_store<DPT>(cnt + w * RADIX + tid * DPT, c);
             }
         }
         __syncthreads();
@@ -537,7 +582,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_onesweep(SweepArgs<
             scatter(std::false_type{});
         }
         // clear the counters for the next tile (no one reads them past step 3)
-        for (int i = tid; i < RANK_WARPS * RADIX; i += THREADS) cnt[i] = 0;
+        zero_counters<RANK_WARPS * RADIX, THREADS>(cnt, tid);
     };
     auto run_tile = [&](int t, int b) {
         const bool full = a.portion_begin + (size_t)(t + 1) * TILE <= portion_end;

@@ -1,9 +1,11 @@
 // ts_tune.cu — the autotuner of the plain LSD and the tuning cache.
 //
-// ts_lsd_autotune times every tile variant of the onesweep pass (keys a
-// thread 22/11/5 for 4-byte keys, 11/5/2 for 8-byte, 32/16/8 for 2-byte) on
-// device-made random keys of one length per length bin, and keeps the fastest
-// per key width and bin in the context. ts_ctx_tune_save / _load keep those
+// ts_lsd_autotune times every tile variant of the 8-bit onesweep pass (keys a
+// thread 22/11/5 for 4-byte keys, 11/5/2 for 8-byte, 32/16/8 for 2-byte) and
+// the 9-, 10- and 11-bit digit widths on device-made random keys of one
+// length per length bin, and keeps the fastest per key width and bin in the
+// context. Widths below 8 bits are not timed: on full-width keys they never
+// need fewer passes than bytes do (ts_lsd_digit_bits still sets them). ts_ctx_tune_save / _load keep those
 // choices, and the segmented sort's per-bin methods, in a JSON file keyed by
 // the GPU's name, so a process can skip the measurement on a GPU it has
 // tuned before.
@@ -34,6 +36,9 @@ __global__ void k_tune_keys(U* d, size_t n, unsigned long long seed) {
     }
 }
 
+// timed per length bin: the 8-bit tile variants, then 9-, 10- and 11-bit digits
+constexpr int LSD_TUNE_CANDIDATES = LSD_VARIANTS + 3;
+
 // the representative length of each bin
 size_t bin_length(int bin, size_t key_bytes) {
     if (bin == 0) return (size_t)1 << 20;
@@ -57,9 +62,13 @@ ts_status tune(ts_ctx* c, float* ms_out) {
         U* d = (U*)((char*)c->gather.p + (n * sizeof(U) + 255) / 256 * 256);
         k_tune_keys<U><<<c->sm_count * 4, 256, 0, c->stream>>>(master, n, 0x243F6A8885A308D3ull + bin);
         float best = 1e30f;
-        int best_v = c->lsd_variant[w][bin];
-        for (int v = 0; v < LSD_VARIANTS && s == TS_OK; ++v) {
-            c->lsd_variant[w][bin] = v;
+        int best_v = c->lsd_variant[w][bin], best_b = c->lsd_bits[w][bin];
+        // candidates: the 8-bit tile variants, then the wider digits (their own tile)
+        for (int v = 0; v < LSD_TUNE_CANDIDATES && s == TS_OK; ++v) {
+            const int cand_v = v < LSD_VARIANTS ? v : 0;
+            const int cand_b = v < LSD_VARIANTS ? 8 : 8 + (v - LSD_VARIANTS + 1);
+            c->lsd_variant[w][bin] = cand_v;
+            c->lsd_bits[w][bin] = cand_b;
             std::vector<float> t;
             for (int rep = 0; rep < 6 && s == TS_OK; ++rep) {
                 cudaMemcpyAsync(d, master, n * sizeof(U), cudaMemcpyDeviceToDevice, c->stream);
@@ -74,13 +83,15 @@ ts_status tune(ts_ctx* c, float* ms_out) {
             if (t.empty()) break;
             std::sort(t.begin(), t.end());
             const float med = t[t.size() / 2];
-            if (ms_out) ms_out[bin * LSD_VARIANTS + v] = med;
+            if (ms_out) ms_out[bin * LSD_TUNE_CANDIDATES + v] = med;
             if (med < best) {
                 best = med;
-                best_v = v;
+                best_v = cand_v;
+                best_b = cand_b;
             }
         }
         c->lsd_variant[w][bin] = best_v;
+        c->lsd_bits[w][bin] = best_b;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -151,6 +162,22 @@ ts_status ts_lsd_variants(ts_ctx* c, size_t key_bytes, int* variants, int set) {
     return TS_OK;
 }
 
+ts_status ts_lsd_digit_bits(ts_ctx* c, size_t key_bytes, int* bits, int set) {
+    if (!c || !bits || (key_bytes != 2 && key_bytes != 4 && key_bytes != 8)) return TS_ERR_INVALID;
+    const int w = width_slot(key_bytes);
+    for (int b = 0; b < LSD_BINS; ++b) {
+        if (set) {
+            if (bits[b] < LSD_MIN_BITS || bits[b] > LSD_MAX_BITS)
+                return fail(c, TS_ERR_INVALID, "digit width outside 4..11 bits");
+        } else {
+            bits[b] = c->lsd_bits[w][b];
+        }
+    }
+    if (set)
+        for (int b = 0; b < LSD_BINS; ++b) c->lsd_bits[w][b] = bits[b];
+    return TS_OK;
+}
+
 int ts_lsd_variant_ipt(size_t key_bytes, int variant) {
     if (variant < 0 || variant >= LSD_VARIANTS) return 0;
     switch (key_bytes) {
@@ -179,6 +206,12 @@ ts_status ts_ctx_tune_save(ts_ctx* c, const char* path) {
     for (int i = 0; i < 4; ++i) {
         const int* m = c->seg_methods[i];
         std::fprintf(f, "%s\"%d\": [%d, %d, %d, %d]", i ? ", " : "", sb[i], m[0], m[1], m[2], m[3]);
+    }
+    std::fprintf(f, "},\n  \"lsd_bits\": {");
+    for (int i = 0; i < 3; ++i) {
+        const int w = width_slot((size_t)wb[i]);
+        std::fprintf(f, "%s\"%d\": [%d, %d, %d]", i ? ", " : "", wb[i], c->lsd_bits[w][0], c->lsd_bits[w][1],
+                     c->lsd_bits[w][2]);
     }
     std::fprintf(f, "}\n}\n");
     const bool ok = std::fclose(f) == 0;
@@ -209,13 +242,27 @@ ts_status ts_ctx_tune_load(ts_ctx* c, const char* path, int* loaded) {
     for (auto& row : lsd)
         for (int v : row)
             if (v < 0 || v >= LSD_VARIANTS) return fail(c, TS_ERR_INVALID, "tuning file: unknown variant");
+    // digit widths (absent from files written before they were tuned: 8 bits)
+    int lbits[3][LSD_BINS];
+    for (auto& row : lbits)
+        for (int& b : row) b = 8;
+    const size_t bp = t.find("\"lsd_bits\":");
+    if (bp != std::string::npos)
+        for (int i = 0; i < 3; ++i)
+            if (!read_array(t, bp, wk[i], lbits[i], LSD_BINS)) return fail(c, TS_ERR_INVALID, "malformed tuning file");
+    for (auto& row : lbits)
+        for (int b : row)
+            if (b < LSD_MIN_BITS || b > LSD_MAX_BITS) return fail(c, TS_ERR_INVALID, "tuning file: digit width");
     const int sbytes[4] = {1, 2, 4, 8};
     for (int i = 0; i < 4; ++i)
         for (int b = 0; b < 4; ++b)
             if (!seg_method_ok(b, seg[i][b], sbytes[i])) return fail(c, TS_ERR_INVALID, "tuning file: unknown method");
     const int wb[3] = {2, 4, 8};
     for (int i = 0; i < 3; ++i)
-        for (int b = 0; b < LSD_BINS; ++b) c->lsd_variant[width_slot((size_t)wb[i])][b] = lsd[i][b];
+        for (int b = 0; b < LSD_BINS; ++b) {
+            c->lsd_variant[width_slot((size_t)wb[i])][b] = lsd[i][b];
+            c->lsd_bits[width_slot((size_t)wb[i])][b] = lbits[i][b];
+        }
     for (int i = 0; i < 4; ++i)
         for (int b = 0; b < 4; ++b) c->seg_methods[i][b] = seg[i][b];
     if (loaded) *loaded = 1;
