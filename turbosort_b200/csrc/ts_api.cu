@@ -52,7 +52,11 @@ int occupancy_of(const void* kernel, int threads, size_t smem) {
     std::lock_guard<std::mutex> g(mu);
     auto it = cache.find(kernel);
     if (it != cache.end()) return it->second;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the default limit (48 KB) covers static and dynamic shared memory together
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) cudaGetLastError();
+    if (smem + fa.sharedSizeBytes > 48 * 1024)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int blocks = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem);
     if (blocks < 1) blocks = 1;
