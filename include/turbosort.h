@@ -88,7 +88,9 @@ unsigned long long ts_ctx_launches(const ts_ctx *ctx);
 /* What the context's last plain sort did (device or host entry point, or a
  * chunk of a host-slice sort); waits for the context's stream. tier: 0 none
  * yet, 1 the small-slice network (n <= 4096), 2 the one-byte counting sort,
- * 3 the LSD passes. For tier 3: mode 0 sorted by passes, 1 input already
+ * 3 the LSD passes, 4 the LSD passes in one cooperative launch (2- and 4-byte
+ * keys whose tiles fit one wave, about 3.3M keys on a B200). For tiers 3 and
+ * 4: mode 0 sorted by passes, 1 input already
  * ascending, 2 descending input reversed; passes and pass_digit[] (8-bit
  * digit indices, least significant first) are the scatter passes that ran;
  * divert_shift > 0 means the sort diverted (src/radix/divert.rs:38-81): only
@@ -106,12 +108,20 @@ ts_status ts_ctx_last_sort_info(ts_ctx *ctx, ts_sort_info *info);
  * digit gets a pass; the output is the same. For comparisons. */
 ts_status ts_ctx_set_divert(ts_ctx *ctx, int on);
 
+/* The single-launch LSD (on by default): a keys-only sort of 2- or 4-byte keys
+ * whose tiles all fit one wave of CTAs (two an SM) runs every step in one
+ * cooperative launch, with bounded grid barriers in place of the look-back.
+ * Off, such sorts take the multi-launch LSD; the output is the same. */
+ts_status ts_ctx_set_single_launch(ts_ctx *ctx, int on);
+
 /* Test hook for failure detection, no counterpart in the crate: in the next
  * LSD sort on this context (keys or order, more than 4096 keys), the first
  * scatter pass's tile 0 never publishes its look-back entry, and every wait
- * on it gives up after spin_limit rounds (normally about a million). The
- * sort then reports TS_ERR_TIMEOUT with every write kept inside the output
- * and scratch buffers; the context stays usable. 0 disarms it. */
+ * on it gives up after spin_limit rounds (normally about a million); in a
+ * single-launch sort, CTA 0 never arrives at the first grid barrier, and
+ * every CTA's wait there gives up the same way. The sort then reports
+ * TS_ERR_TIMEOUT with every write kept inside the output and scratch
+ * buffers; the context stays usable. 0 disarms it. */
 ts_status ts_ctx_test_stall_lookback(ts_ctx *ctx, uint32_t spin_limit);
 
 /* The diverting rule of the crate (src/radix/divert.rs:38-54) as the device

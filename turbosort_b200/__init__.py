@@ -189,6 +189,8 @@ def lib() -> ctypes.CDLL:
             L.ts_ctx_tune_load.restype = st
             L.ts_ctx_set_divert.argtypes = [vp, i]
             L.ts_ctx_set_divert.restype = st
+            L.ts_ctx_set_single_launch.argtypes = [vp, i]
+            L.ts_ctx_set_single_launch.restype = st
             L.ts_ctx_test_stall_lookback.argtypes = [vp, ctypes.c_uint32]
             L.ts_ctx_test_stall_lookback.restype = st
             L.ts_divert_skippable_digits.argtypes = [i, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
@@ -294,6 +296,11 @@ class Context:
         loaded = ctypes.c_int(0)
         self._check(lib().ts_ctx_tune_load(self._h, os.fsencode(path), ctypes.byref(loaded)))
         return bool(loaded.value)
+
+    def set_single_launch(self, on: bool) -> None:
+        """Sorts of 2- and 4-byte keys whose tiles fit one wave run in one
+        cooperative launch (on by default); off, they take the multi-launch LSD."""
+        self._check(lib().ts_ctx_set_single_launch(self._h, int(on)))
 
     def set_divert(self, on: bool) -> None:
         """Diverting of 8-byte keys (on by default); off, every live digit gets a pass."""

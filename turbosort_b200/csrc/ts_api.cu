@@ -416,7 +416,7 @@ ts_status ts_ctx_last_sort_info(ts_ctx* c, ts_sort_info* info) {
     if (!c || !info) return TS_ERR_INVALID;
     std::memset(info, 0, sizeof *info);
     info->tier = c->last_tier;
-    if (c->last_tier != 3 || !c->meta.p) return TS_OK;
+    if ((c->last_tier != 3 && c->last_tier != 4) || !c->meta.p) return TS_OK;
     Plan p{};
     const MetaLayout m = MetaLayout::make(1, 1, 0);  // the plan's place does not depend on the sort
     TS_CUDA(c, cudaMemcpyAsync(&p, (const char*)c->meta.p + m.plan_off, sizeof p, cudaMemcpyDeviceToHost, c->stream));
@@ -432,6 +432,12 @@ ts_status ts_ctx_last_sort_info(ts_ctx* c, ts_sort_info* info) {
 ts_status ts_ctx_set_divert(ts_ctx* c, int on) {
     if (!c) return TS_ERR_INVALID;
     c->divert = on != 0;
+    return TS_OK;
+}
+
+ts_status ts_ctx_set_single_launch(ts_ctx* c, int on) {
+    if (!c) return TS_ERR_INVALID;
+    c->coop = on != 0;
     return TS_OK;
 }
 

@@ -1,0 +1,324 @@
+// ts_coop.cuh — the whole LSD sort of a short slice in one cooperative launch.
+//
+// The crate's LSD (src/radix/mod.rs:180-271): varying bits and sortedness
+// (src/radix/histogram.rs:55-68, src/presorted.rs:15-65), every digit's
+// histogram in one read (src/radix/histogram.rs:15-110), live passes
+// (src/radix/mod.rs:229-239), one stable scatter per live digit
+// (src/radix/scatter.rs:26-247) and the copy back after an odd pass count.
+//
+// A multi-launch sort of 2^20 keys is bound by latency, not bandwidth: four
+// kernels before the first pass, a launch per pass, and in each pass a
+// decoupled look-back whose inclusive prefixes travel a few tiles per L2
+// round trip. Here every tile of the slice belongs to one resident CTA of a
+// single cooperative launch (at most two CTAs an SM), which keeps its tile
+// and replaces the look-back with two grid barriers per pass:
+//   0. each CTA loads its tile as radix keys, ORs key ^ first key, checks the
+//      order of adjacent keys (including the one before its tile) and counts
+//      every digit; the totals go to global memory; barrier;
+//      every CTA derives the same plan (mode, live digits);
+//   per live digit:
+//   1. (after a barrier, from the second pass on) the CTA loads its tile of
+//      the previous pass's output;
+//   2. per-warp digit counts, the tile's counts published, tile-local starts,
+//      and the keys ranked into a staging tile (stable: warp, item, lane);
+//   3. barrier; CTA c computes the column prefix over tiles of digits
+//      c, c + T, ... ; barrier;
+//   4. each digit's global start = its start in the digit's histogram plus
+//      its column prefix; the staging tile goes out as runs per digit.
+// Every grid barrier is bounded: a wait that runs out sets ERR_TIMEOUT and an
+// abort word that ends every other wait, and the kernel returns.
+#pragma once
+
+#include <type_traits>
+
+#include "ts_common.cuh"
+#include "ts_onesweep.cuh"
+
+namespace ts {
+
+struct CoopState {
+    unsigned int arrive;      // grid barrier arrivals (monotonic within a launch)
+    unsigned int abort;       // set when a wait ran out: every later wait returns at once
+    unsigned int flags;       // SCAN_NOT_ASC | SCAN_NOT_DESC
+    unsigned int pad;
+    unsigned long long diff;  // OR of (radix key ^ first radix key)
+};
+
+template <typename U>
+struct CoopArgs {
+    U* data;              // keys, sorted in place
+    U* alt;               // scratch of n keys
+    size_t n;
+    CoopState* st;        // zeroed before the launch
+    unsigned int* hist;   // [ND][256] digit counts, zeroed before the launch
+    unsigned int* tcnt;   // [tiles][256] this pass's tile counts
+    unsigned int* colp;   // [tiles][256] this pass's column prefixes
+    Plan* plan;           // written by CTA 0, for ts_ctx_last_sort_info
+    uint32_t* error;
+    uint32_t spin_limit;  // barrier rounds without progress before ERR_TIMEOUT
+    int withhold_cta0;    // test hook: CTA 0 never arrives at the first barrier
+};
+
+constexpr int COOP_THREADS = 512;
+constexpr int COOP_WARPS = COOP_THREADS / 32;
+
+template <typename U, int IPT>
+struct CoopSmem {
+    static constexpr int TILE = COOP_THREADS * IPT;
+    static constexpr size_t al(size_t x) { return (x + 127) / 128 * 128; }
+    static constexpr size_t kb_off = 0;                                          // [TILE] U
+    static constexpr size_t sk_off = al(kb_off + (size_t)TILE * sizeof(U));      // [TILE] U staged
+    static constexpr size_t cnt_off = al(sk_off + (size_t)TILE * sizeof(U));     // [16][256] u32
+    static constexpr size_t bins_off = cnt_off + (size_t)COOP_WARPS * 256 * 4;   // [256] u32
+    static constexpr size_t gbase_off = bins_off + 256 * 4;                      // [256] i32
+    static constexpr size_t misc_off = gbase_off + 256 * 4;                      // [64] i32
+    static constexpr size_t bytes = misc_off + 64 * 4;
+};
+
+// Bounded grid barrier (all CTAs resident: a cooperative launch). `target`
+// counts the arrivals this CTA waits for; it grows by the grid size per
+// barrier. Returns false once any wait has run out.
+__device__ __forceinline__ bool coop_barrier(CoopState* st, unsigned int& target, uint32_t limit, uint32_t* error,
+                                             int* flag_s, bool arrive = true) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        target += gridDim.x;
+        int ok = ld_volatile_u32(&st->abort) == 0;
+        if (ok) {
+            __threadfence();  // this CTA's writes before its arrival
+            if (arrive) atomicAdd(&st->arrive, 1u);
+            uint32_t spins = 0;
+            while (ld_volatile_u32(&st->arrive) < target) {
+                if (ld_volatile_u32(&st->abort)) {
+                    ok = 0;
+                    break;
+                }
+                if (++spins > limit) {
+                    atomicOr(error, ERR_TIMEOUT);
+                    atomicExch(&st->abort, 1u);
+                    ok = 0;
+                    break;
+                }
+            }
+            __threadfence();  // the others' writes before this CTA's reads
+        }
+        *flag_s = ok;
+    }
+    __syncthreads();
+    return *flag_s != 0;
+}
+
+// Exclusive prefix of v over the CTA's threads (COOP_THREADS); *total gets
+// the sum. tmp: COOP_WARPS words of shared memory.
+__device__ __forceinline__ uint32_t coop_exclusive_scan(uint32_t v, uint32_t* tmp, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) tmp[warp] = x;
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < COOP_WARPS; ++w) {
+        const uint32_t s = tmp[w];
+        before += w < warp ? s : 0u;
+        all += s;
+    }
+    __syncthreads();
+    *total = all;
+    return before + x - v;
+}
+
+template <typename U, int XF, int IPT>
+__global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
+    static_assert(sizeof(U) == 2 || sizeof(U) == 4, "2- and 4-byte keys");
+    using L = CoopSmem<U, IPT>;
+    constexpr int TILE = L::TILE;
+    constexpr int RADIX = 256;
+    constexpr int ND = (int)sizeof(U);
+    extern __shared__ __align__(128) unsigned char smem[];
+    U* kb = reinterpret_cast<U*>(smem + L::kb_off);
+    U* sk = reinterpret_cast<U*>(smem + L::sk_off);
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(smem + L::cnt_off);
+    uint32_t* bins = reinterpret_cast<uint32_t*>(smem + L::bins_off);
+    int* gbase = reinterpret_cast<int*>(smem + L::gbase_off);
+    int* misc = reinterpret_cast<int*>(smem + L::misc_off);  // [0] barrier flag, [1] live count, [2..] digits
+    uint32_t* tmp = reinterpret_cast<uint32_t*>(misc + 32);  // [16] scan scratch
+    __shared__ unsigned long long red_diff[COOP_WARPS];
+    __shared__ unsigned int red_flags[COOP_WARPS];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int t = blockIdx.x, T = gridDim.x;
+    const size_t n = a.n;
+    const size_t base = (size_t)t * TILE;
+    const int tile_n = (int)min((size_t)TILE, n - base);
+    const uint32_t lt = lanemask_lt();
+    PeerMasks<8> pm;
+    pm.init(lane);
+    unsigned int target = 0;
+
+    // ---- 0. the tile, what varies, sortedness, every digit's counts
+    const U first = to_key<U, XF>(a.data[0]);
+    zero_counters<COOP_WARPS * RADIX, COOP_THREADS>(cnt, tid);
+    __syncthreads();
+    unsigned long long diff = 0;
+    unsigned int flags = 0;
+    for (int i = tid; i < tile_n; i += COOP_THREADS) {
+        const U k = to_key<U, XF>(a.data[base + i]);
+        kb[i] = k;
+        diff |= (unsigned long long)(U)(k ^ first);
+#pragma unroll
+        for (int d = 0; d < ND; ++d) atomicAdd(&cnt[d * RADIX + ((k >> (8 * d)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int i = tid; i < tile_n; i += COOP_THREADS) {
+        if (base + i == 0) continue;
+        const U p = i > 0 ? kb[i - 1] : to_key<U, XF>(a.data[base - 1]);
+        const U k = kb[i];
+        flags |= p > k ? SCAN_NOT_ASC : 0u;
+        flags |= p < k ? SCAN_NOT_DESC : 0u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        diff |= __shfl_xor_sync(0xffffffffu, diff, o);
+        flags |= __shfl_xor_sync(0xffffffffu, flags, o);
+    }
+    if (lane == 0) {
+        red_diff[warp] = diff;
+        red_flags[warp] = flags;
+    }
+    for (int i = tid; i < ND * RADIX; i += COOP_THREADS)
+        if (cnt[i]) atomicAdd(&a.hist[i], cnt[i]);
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < COOP_WARPS; ++w) {
+            diff |= red_diff[w];
+            flags |= red_flags[w];
+        }
+        if (diff) atomicOr(&a.st->diff, diff);
+        if (flags) atomicOr(&a.st->flags, flags);
+    }
+    if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc, !(a.withhold_cta0 && t == 0))) return;
+
+    // the plan, the same in every CTA
+    if (tid == 0) {
+        const unsigned long long gd = ld_volatile_u64(&a.st->diff);
+        const unsigned int gf = ld_volatile_u32(&a.st->flags);
+        int mode = MODE_SORT;
+        if (!(gf & SCAN_NOT_ASC)) mode = MODE_SORTED;
+        else if (!(gf & SCAN_NOT_DESC)) mode = MODE_REVERSE;
+        int m = 0;
+        if (mode == MODE_SORT)
+            for (int d = 0; d < ND; ++d)
+                if (((gd >> (8 * d)) & 255ull) && ld_volatile_u32(&a.hist[d * RADIX + ((first >> (8 * d)) & 255u)]) < n)
+                    misc[2 + m++] = d;
+        misc[1] = mode == MODE_SORT ? m : -mode;
+        if (t == 0) {
+            a.plan->mode = mode;
+            a.plan->n_live = m;
+            for (int j = 0; j < m; ++j) a.plan->pass[j] = misc[2 + j];
+            a.plan->divert_shift = 0;
+        }
+    }
+    __syncthreads();
+    const int m = misc[1];
+    if (m == -MODE_REVERSE) {  // descending input: reversed in place (pairs never span two CTAs' ranges)
+        for (size_t i = base + tid; i < base + tile_n && i < n / 2; i += COOP_THREADS) {
+            const U x = a.data[i];
+            a.data[i] = a.data[n - 1 - i];
+            a.data[n - 1 - i] = x;
+        }
+        return;
+    }
+    if (m <= 0) return;  // already sorted, or nothing varies
+
+    const int wbase = warp * 32 * IPT + lane;
+    for (int j = 0; j < m; ++j) {
+        const int shift = 8 * misc[2 + j];
+        const bool last = j == m - 1;
+        U* dst = (j & 1) ? a.data : a.alt;
+        auto dig = [&](U k) -> uint32_t { return __byte_perm((uint32_t)k, 0u, 0x4440u | (uint32_t)(shift >> 3)); };
+
+        // ---- 1. the previous pass's output (written by other CTAs: past L1)
+        if (j > 0) {
+            if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
+            const U* src = (j & 1) ? a.alt : a.data;
+            for (int i = tid; i < tile_n; i += COOP_THREADS) kb[i] = __ldcg(src + base + i);
+            zero_counters<COOP_WARPS * RADIX, COOP_THREADS>(cnt, tid);
+        } else {
+            zero_counters<COOP_WARPS * RADIX, COOP_THREADS>(cnt, tid);
+        }
+        __syncthreads();
+
+        // ---- 2. per-warp counts, the tile's counts, tile-local starts, ranks
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int idx = wbase + i * 32;
+            if (idx < tile_n) atomicAdd(&cnt[warp * RADIX + dig(kb[idx])], 1u);
+        }
+        __syncthreads();
+        uint32_t tc = 0;
+        if (tid < RADIX) {
+#pragma unroll
+            for (int w = 0; w < COOP_WARPS; ++w) {
+                const uint32_t c = cnt[w * RADIX + tid];
+                cnt[w * RADIX + tid] = tc;
+                tc += c;
+            }
+            a.tcnt[(size_t)t * RADIX + tid] = tc;
+        }
+        uint32_t total;
+        const uint32_t lstart = coop_exclusive_scan(tc, tmp, &total);
+        const uint32_t hv = tid < RADIX ? ld_volatile_u32(&a.hist[misc[2 + j] * RADIX + tid]) : 0u;
+        const uint32_t hstart = coop_exclusive_scan(hv, tmp, &total);
+        if (tid < RADIX) {
+            bins[tid] = hstart;
+#pragma unroll
+            for (int w = 0; w < COOP_WARPS; ++w) cnt[w * RADIX + tid] += lstart;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int idx = wbase + i * 32;
+            const bool valid = idx < tile_n;
+            const U k = kb[valid ? idx : 0];
+            const uint32_t d = dig(k);
+            uint32_t peers = (i % 3 == 0) ? __match_any_sync(0xffffffffu, d) : pm.peers(d);
+            peers &= __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+                const uint32_t c = cnt[warp * RADIX + d];
+                cnt[warp * RADIX + d] = c + __popc(peers);
+                sk[c + __popc(peers & lt)] = k;
+            }
+            __syncwarp();
+        }
+
+        // ---- 3. column prefixes over tiles
+        if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
+        for (int r = t; r < RADIX; r += T) {
+            const uint32_t v = tid < T ? __ldcg(&a.tcnt[(size_t)tid * RADIX + r]) : 0u;
+            const uint32_t e = coop_exclusive_scan(v, tmp, &total);
+            if (tid < T) a.colp[(size_t)tid * RADIX + r] = e;
+        }
+        if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
+
+        // ---- 4. global starts, then runs per digit
+        if (tid < RADIX) gbase[tid] = (int)(bins[tid] + __ldcg(&a.colp[(size_t)t * RADIX + tid])) - (int)lstart;
+        __syncthreads();
+        for (int s = tid; s < tile_n; s += COOP_THREADS) {
+            const U k = sk[s];
+            const int p = gbase[dig(k)] + s;
+            if ((size_t)(unsigned)p < n) dst[p] = last ? from_key<U, XF>(k) : k;
+            else atomicOr(a.error, ERR_BOUNDS);
+        }
+    }
+    if (m & 1) {  // the last pass wrote the scratch: copy back
+        if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
+        for (int i = tid; i < tile_n; i += COOP_THREADS) a.data[base + i] = __ldcg(a.alt + base + i);
+    }
+}
+
+}  // namespace ts

@@ -79,10 +79,14 @@ struct ts_ctx {
 
     // diverting of 8-byte keys (ts_ctx_set_divert), on by default as in the crate
     bool divert = true;
+    // 2- and 4-byte keys whose tiles fit one wave sort in one cooperative
+    // launch (ts_ctx_set_single_launch)
+    bool coop = true;
     // test hook (ts_ctx_test_stall_lookback): the next LSD sort's first pass
     // withholds tile 0's look-back entry and gives up after this many rounds
     uint32_t test_spin_limit = 0;
-    // the tier of the last plain sort (ts_sort_info: 1 small, 2 counting, 3 LSD)
+    // the tier of the last plain sort (ts_sort_info: 1 small, 2 counting, 3 LSD,
+    // 4 LSD in one launch)
     int last_tier = 0;
     int last_bits = 8;  // the last LSD sort's digit width
 

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <type_traits>
 
+#include "ts_coop.cuh"
 #include "ts_ctx.h"
 #include "ts_divert.cuh"
 #include "ts_lsd.cuh"
@@ -259,6 +260,75 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     return TS_OK;
 }
 
+// The whole LSD of a keys-only sort of 2- or 4-byte keys in one cooperative
+// launch (k_lsd_coop), with tiles of IPT keys a thread; false in *ran when the
+// slice has more tiles than CTAs that can be resident at once.
+template <typename U, int XF, int IPT>
+static ts_status run_lsd_coop_ipt(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool* ran) {
+    using L = CoopSmem<U, IPT>;
+    constexpr int ND = (int)sizeof(U);
+    auto kern = k_lsd_coop<U, XF, IPT>;
+    const int occ = std::min(2, occupancy_of((const void*)kern, COOP_THREADS, L::bytes));
+    const size_t tiles = (n + L::TILE - 1) / L::TILE;
+    *ran = false;
+    if (tiles > (size_t)occ * c->sm_count || tiles > (size_t)COOP_THREADS) return TS_OK;
+    // meta: the barrier state, the Plan where every LSD keeps it, the digit
+    // counts, and this pass's tile counts and column prefixes
+    const MetaLayout ml = MetaLayout::make(1, 1, 0);
+    const size_t hist_off = ml.plan_off + 768;
+    const size_t tcnt_off = hist_off + (size_t)ND * 256 * 4;
+    const size_t colp_off = tcnt_off + tiles * 256 * 4;
+    ts_status s;
+    if ((s = grow(c, c->meta, colp_off + tiles * 256 * 4, "sort metadata")) != TS_OK) return s;
+    char* meta = (char*)c->meta.p;
+    mark(c, "single-launch LSD");
+    TS_CUDA(c, cudaMemsetAsync(meta, 0, tcnt_off, c->stream));
+    CoopArgs<U> a{};
+    a.data = d_data;
+    a.alt = d_alt;
+    a.n = n;
+    a.st = (CoopState*)meta;
+    a.hist = (unsigned int*)(meta + hist_off);
+    a.tcnt = (unsigned int*)(meta + tcnt_off);
+    a.colp = (unsigned int*)(meta + colp_off);
+    a.plan = (Plan*)(meta + ml.plan_off);
+    a.error = c->d_error;
+    a.spin_limit = c->test_spin_limit ? c->test_spin_limit : SPIN_LIMIT;
+    a.withhold_cta0 = c->test_spin_limit != 0;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)tiles);
+    cfg.blockDim = dim3(COOP_THREADS);
+    cfg.dynamicSmemBytes = L::bytes;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TS_CUDA(c, cudaLaunchKernelEx(&cfg, kern, a));
+    ++c->launches;
+    c->test_spin_limit = 0;
+    *ran = true;
+    return TS_OK;
+}
+
+// The smallest tile that fits the slice into one wave gives the most CTAs.
+template <typename U, int XF>
+static ts_status run_lsd_coop(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool* ran) {
+    ts_status s = run_lsd_coop_ipt<U, XF, 7>(c, d_data, d_alt, n, ran);
+    if (s != TS_OK || *ran) return s;
+    s = run_lsd_coop_ipt<U, XF, 11>(c, d_data, d_alt, n, ran);
+    if (s != TS_OK || *ran) return s;
+    return run_lsd_coop_ipt<U, XF, 22>(c, d_data, d_alt, n, ran);
+}
+// keys a single-launch sort can take on this GPU (one wave of its largest tiles)
+template <typename U, int XF>
+static size_t coop_capacity(ts_ctx* c) {
+    using L = CoopSmem<U, 22>;
+    const int occ = std::min(2, occupancy_of((const void*)k_lsd_coop<U, XF, 22>, COOP_THREADS, L::bytes));
+    return std::min((size_t)occ * c->sm_count, (size_t)COOP_THREADS) * L::TILE;
+}
+
 // The LSD passes of a keys-only sort of n <= 2^31 - 1 keys at a digit width
 // of LSD_MIN_BITS..LSD_MAX_BITS other than 8 (sorted keys end in d_data or,
 // after an odd pass count, d_alt, as the plan says). Compiled apart from the
@@ -335,9 +405,22 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         // a digit width other than 8 (keys below 2^31 only); it never diverts
         const int bits = n <= (size_t)0x7fffffff ? c->lsd_bits[width_slot(sizeof(U))][lsd_bin(n)] : 8;
         c->last_bits = bits;
+        // 2- and 4-byte keys that fit one wave of tiles: the whole sort in one launch
+        bool coop = false;
+        if constexpr (sizeof(U) == 2 || sizeof(U) == 4) coop = bits == 8 && c->coop && n <= coop_capacity<U, XF>(c);
+        c->last_tier = coop ? 4 : 3;
         auto enqueue = [&]() -> ts_status {
             Plan* plan = nullptr;
             ts_status st;
+            if constexpr (sizeof(U) == 2 || sizeof(U) == 4) {
+                if (coop) {
+                    bool ran = false;
+                    if ((st = run_lsd_coop<U, XF>(c, d_data, d_alt, n, &ran)) != TS_OK) return st;
+                    if (!ran) return fail(c, TS_ERR_INTERNAL, "single-launch sort: more tiles than one wave");
+                    mark(c, "end");
+                    return TS_OK;
+                }
+            }
             if (bits != 8)
                 st = run_lsd_bits<U, XF>(c, bits, d_data, d_alt, n, &plan);
             else if (variant == 1)
@@ -380,7 +463,7 @@ ts_status sort_keys_device(ts_ctx* c, U* d_data, size_t n, U* d_alt) {
         if (!c->use_graphs || !c->stream || c->timing || c->test_spin_limit || cs != cudaStreamCaptureStatusNone)
             return enqueue();
         const size_t key[9] = {sizeof(U) | (size_t)XF << 4 | (size_t)variant << 8 | (size_t)(c->divert ? 1 : 0) << 12 |
-                                   (size_t)bits << 16,
+                                   (size_t)bits << 16 | (size_t)(coop ? 1 : 0) << 24,
                                (size_t)d_data, (size_t)d_alt, n,
                                (size_t)c->meta.p, (size_t)c->lookback.p, (size_t)c->d_error, (size_t)c->alt.p,
                                (size_t)c->runs.p};
