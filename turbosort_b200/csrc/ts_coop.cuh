@@ -296,12 +296,19 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
             __syncwarp();
         }
 
-        // ---- 3. column prefixes over tiles
+        // ---- 3. column prefixes over tiles: this CTA's columns c, c + T, ...
+        // side by side (T threads each; at most 256 + T - 1 values), one scan
+        // with each column's first value subtracted (the counters are free now)
         if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
-        for (int r = t; r < RADIX; r += T) {
-            const uint32_t v = tid < T ? __ldcg(&a.tcnt[(size_t)tid * RADIX + r]) : 0u;
+        {
+            const int ncols = t < RADIX ? (RADIX - 1 - t) / T + 1 : 0;
+            const int q = tid / T, row = tid - q * T;
+            const bool act = q < ncols;
+            const uint32_t v = act ? __ldcg(&a.tcnt[(size_t)row * RADIX + t + q * T]) : 0u;
             const uint32_t e = coop_exclusive_scan(v, tmp, &total);
-            if (tid < T) a.colp[(size_t)tid * RADIX + r] = e;
+            cnt[tid] = e;
+            __syncthreads();
+            if (act) a.colp[(size_t)row * RADIX + t + q * T] = e - cnt[q * T];
         }
         if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
 

@@ -74,6 +74,7 @@ ts_status setup(int device, ts_ctx** out) {
     // the scratch is sized for the largest tiles (fewest look-back entries)
     for (auto& row : c->lsd_variant)
         for (int& v : row) v = 0;
+    c->coop = false;  // the multi-launch LSD, whose metadata fits the scratch
     c->alt.p = base;
     c->alt.cap = kAltBytes;
     c->lookback.p = base + kAltBytes;
