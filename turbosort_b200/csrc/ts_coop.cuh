@@ -36,11 +36,16 @@
 
 namespace ts {
 
+// Grid barrier arrivals go to COOP_CTRS counters (CTA t to counter t mod
+// COOP_CTRS), each on its own 128-byte line, so that a few hundred arrivals do
+// not queue on one address; one warp polls all of them at once.
+constexpr int COOP_CTRS = 16;
+constexpr int COOP_CTR_STRIDE = 32;  // words
+
 struct CoopState {
-    unsigned int arrive;      // grid barrier arrivals (monotonic within a launch)
+    unsigned int arrive[COOP_CTRS * COOP_CTR_STRIDE];  // monotonic within a launch
     unsigned int abort;       // set when a wait ran out: every later wait returns at once
     unsigned int flags;       // SCAN_NOT_ASC | SCAN_NOT_DESC
-    unsigned int pad;
     unsigned long long diff;  // OR of (radix key ^ first radix key)
 };
 
@@ -69,40 +74,52 @@ struct CoopSmem {
     static constexpr size_t kb_off = 0;                                          // [TILE] U
     static constexpr size_t sk_off = al(kb_off + (size_t)TILE * sizeof(U));      // [TILE] U staged
     static constexpr size_t cnt_off = al(sk_off + (size_t)TILE * sizeof(U));     // [16][256] u32
-    static constexpr size_t bins_off = cnt_off + (size_t)COOP_WARPS * 256 * 4;   // [256] u32
-    static constexpr size_t gbase_off = bins_off + 256 * 4;                      // [256] i32
+    static constexpr size_t bins_off = cnt_off + (size_t)COOP_WARPS * 256 * 4;   // [4][256] u32
+    static constexpr size_t gbase_off = bins_off + 4 * 256 * 4;                  // [256] i32
     static constexpr size_t misc_off = gbase_off + 256 * 4;                      // [64] i32
     static constexpr size_t bytes = misc_off + 64 * 4;
 };
 
-// Bounded grid barrier (all CTAs resident: a cooperative launch). `target`
-// counts the arrivals this CTA waits for; it grows by the grid size per
-// barrier. Returns false once any wait has run out.
-__device__ __forceinline__ bool coop_barrier(CoopState* st, unsigned int& target, uint32_t limit, uint32_t* error,
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Bounded grid barrier (all CTAs resident: a cooperative launch). `epoch`
+// counts this CTA's barriers so far (warp 0 keeps it). Arrival: a release
+// fence and one add to this CTA's counter; warp 0 then polls every counter
+// (lane k reads counter k) until each holds epoch x its CTAs, and fences
+// (acquire) before the CTA goes on. Returns false once any wait has run out.
+__device__ __forceinline__ bool coop_barrier(CoopState* st, unsigned int& epoch, uint32_t limit, uint32_t* error,
                                              int* flag_s, bool arrive = true) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        target += gridDim.x;
-        int ok = ld_volatile_u32(&st->abort) == 0;
-        if (ok) {
-            __threadfence();  // this CTA's writes before its arrival
-            if (arrive) atomicAdd(&st->arrive, 1u);
-            uint32_t spins = 0;
-            while (ld_volatile_u32(&st->arrive) < target) {
-                if (ld_volatile_u32(&st->abort)) {
-                    ok = 0;
-                    break;
-                }
-                if (++spins > limit) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        ++epoch;
+        bool ok = __shfl_sync(0xffffffffu, (int)(ld_volatile_u32(&st->abort) == 0), 0) != 0;
+        if (ok && lane == 0 && arrive) {
+            fence_acq_rel_gpu();  // this CTA's writes before its arrival
+            atomicAdd(&st->arrive[(blockIdx.x % COOP_CTRS) * COOP_CTR_STRIDE], 1u);
+        }
+        __syncwarp();
+        const unsigned int mapped = lane < COOP_CTRS ? (gridDim.x + COOP_CTRS - 1 - lane) / COOP_CTRS : 0u;
+        const unsigned int want = epoch * mapped;
+        uint32_t spins = 0;
+        while (ok) {
+            const bool mine = lane >= COOP_CTRS || ld_volatile_u32(&st->arrive[lane * COOP_CTR_STRIDE]) >= want;
+            if (__all_sync(0xffffffffu, mine)) break;
+            if (__any_sync(0xffffffffu, lane == 0 && ld_volatile_u32(&st->abort) != 0)) {
+                ok = false;
+                break;
+            }
+            if (++spins > limit) {
+                if (lane == 0) {
                     atomicOr(error, ERR_TIMEOUT);
                     atomicExch(&st->abort, 1u);
-                    ok = 0;
-                    break;
                 }
+                ok = false;
+                break;
             }
-            __threadfence();  // the others' writes before this CTA's reads
         }
-        *flag_s = ok;
+        fence_acq_rel_gpu();  // the others' writes before this CTA's reads
+        if (lane == 0) *flag_s = ok ? 1 : 0;
     }
     __syncthreads();
     return *flag_s != 0;
@@ -132,6 +149,48 @@ __device__ __forceinline__ uint32_t coop_exclusive_scan(uint32_t v, uint32_t* tm
     return before + x - v;
 }
 
+// The keys [g, g + n) into shared memory, past L1 (other CTAs wrote them);
+// from a 16-byte aligned source by 16-byte loads, all issued before the
+// first store.
+template <typename U, int TILE>
+__device__ __forceinline__ void coop_load(U* kb, const U* g, int n, int tid) {
+    constexpr int VN = 16 / (int)sizeof(U);
+    constexpr int PER = (TILE / VN + COOP_THREADS - 1) / COOP_THREADS;
+    int head = 0;
+    if (((uintptr_t)g & 15) == 0) {
+        const int nv = n / VN;
+        const uint4* g4 = reinterpret_cast<const uint4*>(g);
+        uint4* s4 = reinterpret_cast<uint4*>(kb);
+        uint4 r[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int v = tid + k * COOP_THREADS;
+            if (v < nv) r[k] = __ldcg(g4 + v);
+        }
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int v = tid + k * COOP_THREADS;
+            if (v < nv) s4[v] = r[k];
+        }
+        head = nv * VN;
+    }
+    for (int i = head + tid; i < n; i += COOP_THREADS) kb[i] = __ldcg(g + i);
+}
+
+// The keys of shared memory to [g, g + n), by 16-byte stores where g allows.
+template <typename U>
+__device__ __forceinline__ void coop_store(U* g, const U* kb, int n, int tid) {
+    constexpr int VN = 16 / (int)sizeof(U);
+    int head = 0;
+    if (((uintptr_t)g & 15) == 0) {
+        const int nv = n / VN;
+        for (int v = tid; v < nv; v += COOP_THREADS)
+            reinterpret_cast<uint4*>(g)[v] = reinterpret_cast<const uint4*>(kb)[v];
+        head = nv * VN;
+    }
+    for (int i = head + tid; i < n; i += COOP_THREADS) g[i] = kb[i];
+}
+
 template <typename U, int XF, int IPT>
 __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
     static_assert(sizeof(U) == 2 || sizeof(U) == 4, "2- and 4-byte keys");
@@ -158,7 +217,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
     const uint32_t lt = lanemask_lt();
     PeerMasks<8> pm;
     pm.init(lane);
-    unsigned int target = 0;
+    unsigned int epoch = 0;
 
     // ---- 0. the tile, what varies, sortedness, every digit's counts
     const U first = to_key<U, XF>(a.data[0]);
@@ -166,8 +225,10 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
     __syncthreads();
     unsigned long long diff = 0;
     unsigned int flags = 0;
+    coop_load<U, TILE>(kb, a.data + base, tile_n, tid);
+    __syncthreads();
     for (int i = tid; i < tile_n; i += COOP_THREADS) {
-        const U k = to_key<U, XF>(a.data[base + i]);
+        const U k = to_key<U, XF>(kb[i]);
         kb[i] = k;
         diff |= (unsigned long long)(U)(k ^ first);
 #pragma unroll
@@ -201,7 +262,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
         if (diff) atomicOr(&a.st->diff, diff);
         if (flags) atomicOr(&a.st->flags, flags);
     }
-    if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc, !(a.withhold_cta0 && t == 0))) return;
+    if (!coop_barrier(a.st, epoch, a.spin_limit, a.error, misc, !(a.withhold_cta0 && t == 0))) return;
 
     // the plan, the same in every CTA
     if (tid == 0) {
@@ -235,6 +296,19 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
     }
     if (m <= 0) return;  // already sorted, or nothing varies
 
+    // every digit's start in its histogram (the same in every CTA and pass)
+    {
+        uint32_t hv[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) hv[d] = tid < RADIX ? ld_volatile_u32(&a.hist[d * RADIX + tid]) : 0u;
+        uint32_t total;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            const uint32_t e = coop_exclusive_scan(hv[d], tmp, &total);
+            if (tid < RADIX) bins[d * RADIX + tid] = e;
+        }
+    }
+
     const int wbase = warp * 32 * IPT + lane;
     for (int j = 0; j < m; ++j) {
         const int shift = 8 * misc[2 + j];
@@ -244,9 +318,9 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
 
         // ---- 1. the previous pass's output (written by other CTAs: past L1)
         if (j > 0) {
-            if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
+            if (!coop_barrier(a.st, epoch, a.spin_limit, a.error, misc)) return;
             const U* src = (j & 1) ? a.alt : a.data;
-            for (int i = tid; i < tile_n; i += COOP_THREADS) kb[i] = __ldcg(src + base + i);
+            coop_load<U, TILE>(kb, src + base, tile_n, tid);
             zero_counters<COOP_WARPS * RADIX, COOP_THREADS>(cnt, tid);
         } else {
             zero_counters<COOP_WARPS * RADIX, COOP_THREADS>(cnt, tid);
@@ -272,10 +346,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
         }
         uint32_t total;
         const uint32_t lstart = coop_exclusive_scan(tc, tmp, &total);
-        const uint32_t hv = tid < RADIX ? ld_volatile_u32(&a.hist[misc[2 + j] * RADIX + tid]) : 0u;
-        const uint32_t hstart = coop_exclusive_scan(hv, tmp, &total);
         if (tid < RADIX) {
-            bins[tid] = hstart;
 #pragma unroll
             for (int w = 0; w < COOP_WARPS; ++w) cnt[w * RADIX + tid] += lstart;
         }
@@ -299,7 +370,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
         // ---- 3. column prefixes over tiles: this CTA's columns c, c + T, ...
         // side by side (T threads each; at most 256 + T - 1 values), one scan
         // with each column's first value subtracted (the counters are free now)
-        if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
+        if (!coop_barrier(a.st, epoch, a.spin_limit, a.error, misc)) return;
         {
             const int ncols = t < RADIX ? (RADIX - 1 - t) / T + 1 : 0;
             const int q = tid / T, row = tid - q * T;
@@ -310,10 +381,11 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
             __syncthreads();
             if (act) a.colp[(size_t)row * RADIX + t + q * T] = e - cnt[q * T];
         }
-        if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
+        if (!coop_barrier(a.st, epoch, a.spin_limit, a.error, misc)) return;
 
         // ---- 4. global starts, then runs per digit
-        if (tid < RADIX) gbase[tid] = (int)(bins[tid] + __ldcg(&a.colp[(size_t)t * RADIX + tid])) - (int)lstart;
+        if (tid < RADIX)
+            gbase[tid] = (int)(bins[misc[2 + j] * RADIX + tid] + __ldcg(&a.colp[(size_t)t * RADIX + tid])) - (int)lstart;
         __syncthreads();
         for (int s = tid; s < tile_n; s += COOP_THREADS) {
             const U k = sk[s];
@@ -323,8 +395,10 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
         }
     }
     if (m & 1) {  // the last pass wrote the scratch: copy back
-        if (!coop_barrier(a.st, target, a.spin_limit, a.error, misc)) return;
-        for (int i = tid; i < tile_n; i += COOP_THREADS) a.data[base + i] = __ldcg(a.alt + base + i);
+        if (!coop_barrier(a.st, epoch, a.spin_limit, a.error, misc)) return;
+        coop_load<U, TILE>(kb, a.alt + base, tile_n, tid);
+        __syncthreads();
+        coop_store<U>(a.data + base, kb, tile_n, tid);
     }
 }
 

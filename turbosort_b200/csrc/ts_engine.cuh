@@ -275,7 +275,9 @@ static ts_status run_lsd_coop_ipt(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool
     // meta: the barrier state, the Plan where every LSD keeps it, the digit
     // counts, and this pass's tile counts and column prefixes
     const MetaLayout ml = MetaLayout::make(1, 1, 0);
-    const size_t hist_off = ml.plan_off + 768;
+    const size_t state_off = 1024;  // after the plan area
+    static_assert(sizeof(Plan) + 256 <= 1024, "the plan area ends before the barrier state");
+    const size_t hist_off = (state_off + sizeof(CoopState) + 255) / 256 * 256;
     const size_t tcnt_off = hist_off + (size_t)ND * 256 * 4;
     const size_t colp_off = tcnt_off + tiles * 256 * 4;
     ts_status s;
@@ -287,7 +289,7 @@ static ts_status run_lsd_coop_ipt(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool
     a.data = d_data;
     a.alt = d_alt;
     a.n = n;
-    a.st = (CoopState*)meta;
+    a.st = (CoopState*)(meta + state_off);
     a.hist = (unsigned int*)(meta + hist_off);
     a.tcnt = (unsigned int*)(meta + tcnt_off);
     a.colp = (unsigned int*)(meta + colp_off);
