@@ -88,10 +88,10 @@ unsigned long long ts_ctx_launches(const ts_ctx *ctx);
 /* What the context's last plain sort did (device or host entry point, or a
  * chunk of a host-slice sort); waits for the context's stream. tier: 0 none
  * yet, 1 the small-slice network (n <= 4096), 2 the one-byte counting sort,
- * 3 the LSD passes, 4 the LSD passes in one cooperative launch (2- and 4-byte
- * keys whose tiles fit one wave, about 3.3M keys on a B200). For tiers 3 and
- * 4: mode 0 sorted by passes, 1 input already
- * ascending, 2 descending input reversed; passes and pass_digit[] (8-bit
+ * 3 the LSD passes, 4 the LSD passes in one cooperative launch (2- and
+ * 4-byte keys whose tiles fit one wave, up to 1,667,072 keys on a B200). For
+ * tiers 3 and 4: mode 0 sorted by passes, 1 input already ascending, 2
+ * descending input reversed; passes and pass_digit[] (8-bit
  * digit indices, least significant first) are the scatter passes that ran;
  * divert_shift > 0 means the sort diverted (src/radix/divert.rs:38-81): only
  * the digits from that bit up were sorted by passes, and the runs of keys

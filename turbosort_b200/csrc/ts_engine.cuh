@@ -315,19 +315,22 @@ static ts_status run_lsd_coop_ipt(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool
 }
 
 // The smallest tile that fits the slice into one wave gives the most CTAs.
+// Tiles of 22 keys a thread (one wave of up to 3.3M keys) were slower than
+// the multi-launch sort from 2M keys on (a B200: 0.125 against 0.110 ms at
+// 2^21, whose 187 tiles give 39 SMs two), so the largest tile is 11 keys a
+// thread (1,667,072 keys on 148 SMs).
+constexpr int COOP_MAX_IPT = 11;
 template <typename U, int XF>
 static ts_status run_lsd_coop(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool* ran) {
     ts_status s = run_lsd_coop_ipt<U, XF, 7>(c, d_data, d_alt, n, ran);
     if (s != TS_OK || *ran) return s;
-    s = run_lsd_coop_ipt<U, XF, 11>(c, d_data, d_alt, n, ran);
-    if (s != TS_OK || *ran) return s;
-    return run_lsd_coop_ipt<U, XF, 22>(c, d_data, d_alt, n, ran);
+    return run_lsd_coop_ipt<U, XF, COOP_MAX_IPT>(c, d_data, d_alt, n, ran);
 }
 // keys a single-launch sort can take on this GPU (one wave of its largest tiles)
 template <typename U, int XF>
 static size_t coop_capacity(ts_ctx* c) {
-    using L = CoopSmem<U, 22>;
-    const int occ = std::min(2, occupancy_of((const void*)k_lsd_coop<U, XF, 22>, COOP_THREADS, L::bytes));
+    using L = CoopSmem<U, COOP_MAX_IPT>;
+    const int occ = std::min(2, occupancy_of((const void*)k_lsd_coop<U, XF, COOP_MAX_IPT>, COOP_THREADS, L::bytes));
     return std::min((size_t)occ * c->sm_count, (size_t)COOP_THREADS) * L::TILE;
 }
 
