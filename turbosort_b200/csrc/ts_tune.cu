@@ -49,8 +49,11 @@ size_t bin_length(int bin, size_t key_bytes) {
 template <typename U>
 ts_status tune(ts_ctx* c, float* ms_out) {
     const int w = width_slot(sizeof(U));
-    const bool graphs = c->use_graphs;
+    // the variants serve the multi-launch LSD: single-launch sorts (short
+    // slices) are left out of the timing
+    const bool graphs = c->use_graphs, coop = c->coop;
     c->use_graphs = false;
+    c->coop = false;
     ts_status s = TS_OK;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
@@ -96,6 +99,7 @@ ts_status tune(ts_ctx* c, float* ms_out) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->use_graphs = graphs;
+    c->coop = coop;
     if (s != TS_OK) return s;
     return finish(c);
 }
