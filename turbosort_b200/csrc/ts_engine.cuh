@@ -60,9 +60,6 @@ struct LsdCfg {
     // keys without diverting 6.62 -> 6.47 ms; 2^28 u32 keys 4.22 -> 4.38 ms,
     // so 8-byte keys only
     static constexpr bool LB_PAIR = sizeof(U) == 8 && !PAIRS && B == 8;
-    // the ranking's counter update by one atomic of each equal-digit group's
-    // lowest lane (k_onesweep RANK_ATOM)
-    static constexpr bool RANK_ATOM = false;
     // 8-byte keys without positions divert (src/radix/divert.rs): the plan may
     // leave out the lowest live digits, and k_divert_runs / k_divert_long
     // finish the runs that leaves
@@ -216,11 +213,11 @@ static ts_status run_lsd(ts_ctx* c, const U* in, U* pp0, U* pp1, uint32_t* vpp0,
     {
         using Sm = typename C::Smem;
         auto kern = k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, false, C::MATCH_MOD, C::MATCH_CNT,
-                               C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR, C::RANK_ATOM>;
+                               C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>;
         if constexpr (C::HUGE_OK) {
             if (n > (size_t)0x7fffffff)
                 kern = k_onesweep<U, XF, C::BITS, C::THREADS, C::IPT, PAIRS, C::NBUF, true, C::MATCH_MOD, C::MATCH_CNT,
-                                  C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR, C::RANK_ATOM>;
+                                  C::UNSTABLE1, C::RANK_AHEAD, C::LBW, C::LB_PAIR>;
         } else {
             if (n > (size_t)0x7fffffff) return fail(c, TS_ERR_INTERNAL, "digit width without 64-bit offsets");
         }

@@ -154,8 +154,7 @@ __device__ __forceinline__ void zero_counters(uint32_t* cnt, int tid) {
 // equal in every bit are the same bit pattern, so their order is not
 // observable. With positions (PAIRS) every pass stays stable.
 template <typename U, int XF, int BITS, int THREADS, int IPT, bool PAIRS, int NBUF, bool BIG, int MATCH_MOD,
-          int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false, int LBW = LB_WINDOW, bool LB_PAIR = false,
-          bool RANK_ATOM = false>
+          int MATCH_CNT, bool UNSTABLE1 = false, bool RANK_AHEAD = false, int LBW = LB_WINDOW, bool LB_PAIR = false>
 __global__ void __launch_bounds__(THREADS, SweepSmem<U, BITS, THREADS, IPT, PAIRS, NBUF, LB_PAIR>::bytes <= 113 * 1024
                                                ? 1024 / THREADS
                                                : 1) k_onesweep(SweepArgs<U, PAIRS> a) {
@@ -396,26 +395,12 @@ __global__ void __launch_bounds__(THREADS, SweepSmem<U, BITS, THREADS, IPT, PAIR
                 const U k = kn;
                 const uint32_t d = dn, peers = pn;
                 if (i + 1 < IPT) find(i + 1, kn, dn, pn);
-                if constexpr (RANK_ATOM) {
-                    // the lowest lane of each equal-digit group moves the
-                    // counter with one atomic and hands the old count on
-                    const int leader = __ffs(peers) - 1;
-                    uint32_t old = 0;
-                    if ((FULL || idx < tile_n) && lane == leader) old = atomicAdd(&my_cnt[d], (uint32_t)__popc(peers));
-                    const uint32_t c = __shfl_sync(0xffffffffu, old, leader & 31);
-                    if (FULL || idx < tile_n) {
-                        const uint32_t pos = c + __popc(peers & lt);
-                        sk[pos] = k;
-                        if constexpr (PAIRS) sv[pos] = FIRST ? (uint32_t)(tile_base + idx) : vb[idx];
-                    }
-                } else {
-                    if (FULL || idx < tile_n) {
-                        const uint32_t c = my_cnt[d];
-                        my_cnt[d] = c + __popc(peers);
-                        const uint32_t pos = c + __popc(peers & lt);
-                        sk[pos] = k;
-                        if constexpr (PAIRS) sv[pos] = FIRST ? (uint32_t)(tile_base + idx) : vb[idx];
-                    }
+                if (FULL || idx < tile_n) {
+                    const uint32_t c = my_cnt[d];
+                    my_cnt[d] = c + __popc(peers);
+                    const uint32_t pos = c + __popc(peers & lt);
+                    sk[pos] = k;
+                    if constexpr (PAIRS) sv[pos] = FIRST ? (uint32_t)(tile_base + idx) : vb[idx];
                 }
                 __syncwarp();
             }
