@@ -262,7 +262,7 @@ typedef struct ts_learned_params {
                                 histograms, diverting included; keys of at most this many bytes
                                 need no estimate), the plain sort runs instead (reason 4);
                                 0 = never */
-    int32_t verify;          /* the judge: 1 = sort a copy with the plain LSD as well and count
+    int32_t verify;          /* 1 = sort a copy with the plain LSD as well and count
                                 the keys where the outputs differ (stats->verify_mismatches);
                                 any difference returns TS_ERR_INTERNAL */
 } ts_learned_params;
@@ -278,7 +278,7 @@ typedef struct ts_learned_stats {
                            4 routed: the plain sort's estimated passes <= route_passes */
     float ms_sample, ms_train, ms_partition, ms_buckets;
     int32_t est_plain_passes;     /* the plain sort's estimated scatter passes (-1: not estimated) */
-    int32_t verified;             /* 1: the judge compared the output with the plain sort's */
+    int32_t verified;             /* 1: the verify pass compared the output with the plain sort's */
     uint64_t verify_mismatches;   /* keys where they differ (0 when correct) */
     float ms_verify;
     float pad;

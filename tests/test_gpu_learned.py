@@ -321,7 +321,7 @@ def test_cost_route(ts, W, kind, n, routed):
 
 
 @pytest.mark.parametrize("kind", ["lognormal_f64", "gauss_mix_u64", "unit_f32_dups", "specials_f64"])
-def test_judge_compares_with_the_plain_sort(ts, W, kind):
+def test_verify_compares_with_the_plain_sort(ts, W, kind):
     """verify = 1: the plain LSD sorts a copy on the device and the outputs
     are compared key for key; a good model and a corrupted one both agree."""
     a = inputs(W, kind, seed=33)

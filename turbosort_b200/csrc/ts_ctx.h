@@ -39,7 +39,7 @@ struct ts_ctx {
     ts::DevBuf gather;             // apply_order staging
     ts::DevBuf seg;                // segmented sort: plan, work counter, bin lists, offsets
     ts::DevBuf learn;              // learned partition: sample, model, training state, bucket counts
-    ts::DevBuf check;              // learned partition's judge: a copy of the keys, sorted by the plain LSD
+    ts::DevBuf check;              // learned partition's verify pass: a copy of the keys, sorted by the plain LSD
     ts::DevBuf pipe;               // host-slice pipeline: merge split points
     ts::DevBuf pipe_pos[2];        // host-slice pipeline of sort_by_key: position runs
     uint32_t* d_error = nullptr;   // kernel-reported errors, read and cleared by the host

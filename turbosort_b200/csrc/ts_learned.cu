@@ -32,7 +32,7 @@ struct LmBuffers {
     LmTables T;
     double* loss;  // [2]: before the first step, after the last
     float* max_err;
-    unsigned long long* mismatches;  // the judge's count
+    unsigned long long* mismatches;  // the verify pass's count
     unsigned long long *totals, *offsets, *max_bucket, *cur1, *cur2;
     unsigned int *tiles_before, *counter;
     size_t bytes;
@@ -164,9 +164,9 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     TS_CUDA(c, cudaFuncSetAttribute((const void*)k_lm_finish<U, XF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     MSD_SMEM));
 
-    U* check = nullptr;  // the judge's copy of the input
+    U* check = nullptr;  // the verify pass's copy of the input
     if (prm.verify) {
-        if ((s = grow(c, c->check, n * sizeof(U) + 16, "judge copy")) != TS_OK) return done(s);
+        if ((s = grow(c, c->check, n * sizeof(U) + 16, "verify copy")) != TS_OK) return done(s);
         check = (U*)c->check.p;
         TS_CUDA(c, cudaMemcpyAsync(check, d, n * sizeof(U), cudaMemcpyDeviceToDevice, c->stream));
     }
@@ -295,7 +295,7 @@ static ts_status learned_sort_device(ts_ctx* c, U* d, size_t n, const ts_learned
     TS_CUDA(c, cudaGetLastError());
     cudaEventRecord(ev.e[6], c->stream);
     if (check) {
-        // the judge: the plain LSD sorts the copy, and the outputs must agree
+        // verify: the plain LSD sorts the copy, and the outputs must agree
         // key for key (an exact sort has one output)
         TS_CUDA(c, cudaMemsetAsync(B.mismatches, 0, 8, c->stream));
         if ((s = sort_keys_device<U, XF>(c, check, n, nullptr)) != TS_OK) return done(s);
