@@ -10,23 +10,26 @@
 // kernels before the first pass, a launch per pass, and in each pass a
 // decoupled look-back whose inclusive prefixes travel a few tiles per L2
 // round trip. Here every tile of the slice belongs to one resident CTA of a
-// single cooperative launch (at most two CTAs an SM), which keeps its tile
-// and replaces the look-back with two grid barriers per pass:
+// single cooperative launch (at most two CTAs an SM):
 //   0. each CTA loads its tile as radix keys, ORs key ^ first key, checks the
 //      order of adjacent keys (including the one before its tile) and counts
-//      every digit; the totals go to global memory; barrier;
-//      every CTA derives the same plan (mode, live digits);
+//      every digit; the totals go to global memory; grid barrier;
+//      every CTA derives the same plan (mode, live digits) and every digit's
+//      start in its histogram;
 //   per live digit:
-//   1. (after a barrier, from the second pass on) the CTA loads its tile of
-//      the previous pass's output;
-//   2. per-warp digit counts, the tile's counts published, tile-local starts,
-//      and the keys ranked into a staging tile (stable: warp, item, lane);
-//   3. barrier; CTA c computes the column prefix over tiles of digits
-//      c, c + T, ... ; barrier;
-//   4. each digit's global start = its start in the digit's histogram plus
-//      its column prefix; the staging tile goes out as runs per digit.
-// Every grid barrier is bounded: a wait that runs out sets ERR_TIMEOUT and an
-// abort word that ends every other wait, and the kernel returns.
+//   1. (after a grid barrier, from the second pass on) the CTA loads its
+//      tile of the previous pass's output;
+//   2. per-warp digit counts; the tile's counts are published at once, each
+//      16-bit field tagged with the pass; tile-local starts; the keys ranked
+//      into a staging tile (stable: warp, item, lane);
+//   3. the CTA sums the published counts of every earlier tile (re-reading
+//      a word until all of its fields carry this pass's tag): the keys of
+//      each digit that come before this tile's;
+//   4. each digit's global start = its start in the histogram plus that sum;
+//      the staging tile goes out as runs per digit.
+// Every wait is bounded: a grid barrier or a tag wait that runs out sets
+// ERR_TIMEOUT and an abort word that ends every other wait, and the kernel
+// returns.
 #pragma once
 
 #include <type_traits>
@@ -56,8 +59,7 @@ struct CoopArgs {
     size_t n;
     CoopState* st;        // zeroed before the launch
     unsigned int* hist;   // [ND][256] digit counts, zeroed before the launch
-    unsigned int* tcnt;   // [tiles][256] this pass's tile counts
-    unsigned int* colp;   // [tiles][256] this pass's column prefixes
+    unsigned short* tcnt; // [tiles][256] tile counts: (pass + 1) << 13 | count, zeroed before the launch
     Plan* plan;           // written by CTA 0, for ts_ctx_last_sort_info
     uint32_t* error;
     uint32_t spin_limit;  // barrier rounds without progress before ERR_TIMEOUT
@@ -66,6 +68,16 @@ struct CoopArgs {
 
 constexpr int COOP_THREADS = 512;
 constexpr int COOP_WARPS = COOP_THREADS / 32;
+// a published tile count: 13 bits of count under a 3-bit pass tag
+constexpr int COOP_COUNT_BITS = 13;
+constexpr uint32_t COOP_COUNT_MASK = (1u << COOP_COUNT_BITS) - 1;
+
+// all eight 16-bit fields of w carry `tag`
+__device__ __forceinline__ bool coop_tagged(const uint4& w, unsigned int tag) {
+    const uint32_t t2 = tag << COOP_COUNT_BITS | tag << (16 + COOP_COUNT_BITS);
+    const uint32_t m = ~(COOP_COUNT_MASK | COOP_COUNT_MASK << 16);
+    return ((w.x & m) == t2) & ((w.y & m) == t2) & ((w.z & m) == t2) & ((w.w & m) == t2);
+}
 
 template <typename U, int IPT>
 struct CoopSmem {
@@ -196,6 +208,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
     static_assert(sizeof(U) == 2 || sizeof(U) == 4, "2- and 4-byte keys");
     using L = CoopSmem<U, IPT>;
     constexpr int TILE = L::TILE;
+    static_assert(TILE <= (int)COOP_COUNT_MASK && (int)sizeof(U) < 8, "a tile's counts and pass tags fit 16 bits");
     constexpr int RADIX = 256;
     constexpr int ND = (int)sizeof(U);
     extern __shared__ __align__(128) unsigned char smem[];
@@ -342,7 +355,7 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
                 cnt[w * RADIX + tid] = tc;
                 tc += c;
             }
-            a.tcnt[(size_t)t * RADIX + tid] = tc;
+            a.tcnt[(size_t)t * RADIX + tid] = (unsigned short)((unsigned)(j + 1) << COOP_COUNT_BITS | tc);
         }
         uint32_t total;
         const uint32_t lstart = coop_exclusive_scan(tc, tmp, &total);
@@ -367,25 +380,61 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
             __syncwarp();
         }
 
-        // ---- 3. column prefixes over tiles: this CTA's columns c, c + T, ...
-        // side by side (T threads each; at most 256 + T - 1 values), one scan
-        // with each column's first value subtracted (the counters are free now)
-        if (!coop_barrier(a.st, epoch, a.spin_limit, a.error, misc)) return;
+        // ---- 3. each digit's keys in earlier tiles: the sum of their
+        // published counts. Thread (g, q) reads uint4 column q (digits 8q ..
+        // 8q + 7) of rows g, g + 16, ..., re-reading a word until all of its
+        // fields carry this pass's tag; the 16 row groups meet in the counters.
         {
-            const int ncols = t < RADIX ? (RADIX - 1 - t) / T + 1 : 0;
-            const int q = tid / T, row = tid - q * T;
-            const bool act = q < ncols;
-            const uint32_t v = act ? __ldcg(&a.tcnt[(size_t)row * RADIX + t + q * T]) : 0u;
-            const uint32_t e = coop_exclusive_scan(v, tmp, &total);
-            cnt[tid] = e;
+            const int q = tid & 31, g = tid >> 5;
+            const uint4* rows = reinterpret_cast<const uint4*>(a.tcnt);
+            const unsigned int tag = (unsigned int)(j + 1);
+            uint32_t part[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            bool ok = true;
+            uint32_t spins = 0;
+            constexpr int INFLIGHT = 6;
+            for (int r0 = g; r0 < t && ok; r0 += 16 * INFLIGHT) {
+                uint4 v[INFLIGHT];
+#pragma unroll
+                for (int u = 0; u < INFLIGHT; ++u) {
+                    const int r = r0 + 16 * u;
+                    if (r < t) v[u] = __ldcv(rows + (size_t)r * 32 + q);
+                }
+#pragma unroll
+                for (int u = 0; u < INFLIGHT; ++u) {
+                    const int r = r0 + 16 * u;
+                    if (r >= t || !ok) continue;
+                    while (!coop_tagged(v[u], tag)) {
+                        if (++spins > a.spin_limit) {
+                            ok = false;
+                            break;
+                        }
+                        v[u] = __ldcv(rows + (size_t)r * 32 + q);
+                    }
+                    const uint32_t w[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        part[2 * e] += w[e] & COOP_COUNT_MASK;
+                        part[2 * e + 1] += (w[e] >> 16) & COOP_COUNT_MASK;
+                    }
+                }
+            }
+            if (!ok) {
+                atomicOr(a.error, ERR_TIMEOUT);
+                atomicExch(&a.st->abort, 1u);
+            }
+            if (__syncthreads_or(!ok)) return;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) cnt[g * RADIX + 8 * q + e] = part[e];
             __syncthreads();
-            if (act) a.colp[(size_t)row * RADIX + t + q * T] = e - cnt[q * T];
         }
-        if (!coop_barrier(a.st, epoch, a.spin_limit, a.error, misc)) return;
 
         // ---- 4. global starts, then runs per digit
-        if (tid < RADIX)
-            gbase[tid] = (int)(bins[misc[2 + j] * RADIX + tid] + __ldcg(&a.colp[(size_t)t * RADIX + tid])) - (int)lstart;
+        if (tid < RADIX) {
+            uint32_t before = 0;
+#pragma unroll
+            for (int g = 0; g < COOP_WARPS; ++g) before += cnt[g * RADIX + tid];
+            gbase[tid] = (int)(bins[misc[2 + j] * RADIX + tid] + before) - (int)lstart;
+        }
         __syncthreads();
         for (int s = tid; s < tile_n; s += COOP_THREADS) {
             const U k = sk[s];

@@ -272,27 +272,26 @@ static ts_status run_lsd_coop_ipt(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool
     const size_t tiles = (n + L::TILE - 1) / L::TILE;
     *ran = false;
     if (tiles > (size_t)occ * c->sm_count || tiles > (size_t)COOP_THREADS) return TS_OK;
-    // meta: the barrier state, the Plan where every LSD keeps it, the digit
-    // counts, and this pass's tile counts and column prefixes
+    // meta: the Plan where every LSD keeps it, the barrier state, the digit
+    // counts and the tile counts (zeroed: no pass's tag)
     const MetaLayout ml = MetaLayout::make(1, 1, 0);
     const size_t state_off = 1024;  // after the plan area
     static_assert(sizeof(Plan) + 256 <= 1024, "the plan area ends before the barrier state");
     const size_t hist_off = (state_off + sizeof(CoopState) + 255) / 256 * 256;
     const size_t tcnt_off = hist_off + (size_t)ND * 256 * 4;
-    const size_t colp_off = tcnt_off + tiles * 256 * 4;
+    const size_t end = tcnt_off + tiles * 256 * 2;
     ts_status s;
-    if ((s = grow(c, c->meta, colp_off + tiles * 256 * 4, "sort metadata")) != TS_OK) return s;
+    if ((s = grow(c, c->meta, end, "sort metadata")) != TS_OK) return s;
     char* meta = (char*)c->meta.p;
     mark(c, "single-launch LSD");
-    TS_CUDA(c, cudaMemsetAsync(meta, 0, tcnt_off, c->stream));
+    TS_CUDA(c, cudaMemsetAsync(meta, 0, end, c->stream));
     CoopArgs<U> a{};
     a.data = d_data;
     a.alt = d_alt;
     a.n = n;
     a.st = (CoopState*)(meta + state_off);
     a.hist = (unsigned int*)(meta + hist_off);
-    a.tcnt = (unsigned int*)(meta + tcnt_off);
-    a.colp = (unsigned int*)(meta + colp_off);
+    a.tcnt = (unsigned short*)(meta + tcnt_off);
     a.plan = (Plan*)(meta + ml.plan_off);
     a.error = c->d_error;
     a.spin_limit = c->test_spin_limit ? c->test_spin_limit : SPIN_LIMIT;
