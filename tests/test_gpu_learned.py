@@ -320,6 +320,24 @@ def test_cost_route(ts, W, kind, n, routed):
         assert st["reason"] != 4 and st["est_plain_passes"] >= 5, st
 
 
+@pytest.mark.parametrize("bits, passes", [(32, 4), (16, 2)])
+def test_route_estimate_from_a_short_sample(ts, W, bits, passes):
+    """With route_passes = 3, 4-byte keys are sampled and the estimate comes
+    from the plain sort of the sample (21K keys here: the single-launch
+    sort), which must report each live digit's largest bucket: random u32
+    keys need four passes (the partition runs), keys of 16 varying bits two
+    (routed to the plain sort)."""
+    import turbosort_b200 as real
+
+    rng = np.random.default_rng(bits)
+    a = (rng.integers(0, 2**32, size=N, dtype=np.uint64) & np.uint64((1 << bits) - 1)).astype(np.uint32)
+    got = a.copy()
+    st = real.sort_learned(got, route_passes=3)
+    same_bits(got, O.sort(a))
+    assert st["est_plain_passes"] == passes, st
+    assert (st["reason"] == 4) == (passes <= 3), st
+
+
 @pytest.mark.parametrize("kind", ["lognormal_f64", "gauss_mix_u64", "unit_f32_dups", "specials_f64"])
 def test_verify_compares_with_the_plain_sort(ts, W, kind):
     """verify = 1: the plain LSD sorts a copy on the device and the outputs

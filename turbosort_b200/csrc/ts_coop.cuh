@@ -61,6 +61,7 @@ struct CoopArgs {
     unsigned int* hist;   // [ND][256] digit counts, zeroed before the launch
     unsigned short* tcnt; // [tiles][256] tile counts: (pass + 1) << 13 | count, zeroed before the launch
     Plan* plan;           // written by CTA 0, for ts_ctx_last_sort_info
+    unsigned long long* maxb;  // [ND] each live digit's largest bucket (0: not live), written by CTA 0
     uint32_t* error;
     uint32_t spin_limit;  // barrier rounds without progress before ERR_TIMEOUT
     int withhold_cta0;    // test hook: CTA 0 never arrives at the first barrier
@@ -298,6 +299,25 @@ __global__ void __launch_bounds__(COOP_THREADS, 2) k_lsd_coop(CoopArgs<U> a) {
         }
     }
     __syncthreads();
+    if (t == 0) {  // each live digit's largest bucket, as the multi-launch plan reports it
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            uint32_t mx = tid < RADIX ? ld_volatile_u32(&a.hist[d * RADIX + tid]) : 0u;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0) tmp[warp] = mx;
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t all = 0;
+                for (int w = 0; w < COOP_WARPS; ++w) all = max(all, tmp[w]);
+                const unsigned long long gd = ld_volatile_u64(&a.st->diff);
+                const bool live = ((gd >> (8 * d)) & 255ull) &&
+                                  ld_volatile_u32(&a.hist[d * RADIX + ((first >> (8 * d)) & 255u)]) < n;
+                a.maxb[d] = live ? all : 0ull;
+            }
+            __syncthreads();
+        }
+    }
     const int m = misc[1];
     if (m == -MODE_REVERSE) {  // descending input: reversed in place (pairs never span two CTAs' ranges)
         for (size_t i = base + tid; i < base + tile_n && i < n / 2; i += COOP_THREADS) {

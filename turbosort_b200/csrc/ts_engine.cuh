@@ -293,6 +293,7 @@ static ts_status run_lsd_coop_ipt(ts_ctx* c, U* d_data, U* d_alt, size_t n, bool
     a.hist = (unsigned int*)(meta + hist_off);
     a.tcnt = (unsigned short*)(meta + tcnt_off);
     a.plan = (Plan*)(meta + ml.plan_off);
+    a.maxb = (unsigned long long*)(meta + ml.maxb_off());
     a.error = c->d_error;
     a.spin_limit = c->test_spin_limit ? c->test_spin_limit : SPIN_LIMIT;
     a.withhold_cta0 = c->test_spin_limit != 0;
