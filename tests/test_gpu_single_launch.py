@@ -125,6 +125,26 @@ def test_same_output_with_the_multi_launch_sort(env):
         ctx.set_single_launch(True)
 
 
+@pytest.mark.parametrize("t", [np.uint16, np.uint32])
+def test_unaligned_keys(env, t):
+    """Keys one element past a 16-byte boundary take the scalar tile loads
+    and stores; the caller's buffer serves as the scratch."""
+    torch, ts, O, ctx = env
+    L = ts.lib()
+    n = 300_007
+    a = _keys(t, n, 11)
+    iview = {2: np.int16, 4: np.int32}[a.dtype.itemsize]
+    big = torch.from_numpy(np.concatenate([np.zeros(1, a.dtype), a]).view(iview).copy()).cuda()
+    buf = torch.empty(n + 1, dtype=big.dtype, device="cuda")
+    w = a.dtype.itemsize
+    fn = getattr(L, f"ts_sort_dev_with_buffer_u{8 * w}")
+    assert fn(ctx.handle, big.data_ptr() + w, n, buf.data_ptr() + w, n) == 0
+    assert L.ts_ctx_synchronize(ctx.handle) == 0
+    assert ctx.last_sort_info()["tier"] == 4
+    got = big.cpu().numpy().view(a.dtype)
+    assert got[0] == 0 and got[1:].tobytes() == O.sort(a).tobytes()
+
+
 def test_graph_replay(env):
     """Repeated calls with the same pointers replay a captured graph."""
     torch, ts, O, _ = env
