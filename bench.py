@@ -806,6 +806,12 @@ def main() -> None:
                         "pass_frac": round(rr["n"] * rr["w"] * 2 / (ow / 1e3) / 1e9 / peak, 3) if ow else None,
                         "ok": rr["ok"]}
         bd["c1_u32_2p20"] = bench_small(ts, torch, ctx, "u32", 0, 20, max(10, args.steps), 5, 0x1234 + rank)
+        bd["c1_u32_2p20"]["tier"] = ctx.last_sort_info()["tier"]
+        # the same sort through the multi-launch LSD, for comparison
+        ctx.set_single_launch(False)
+        bd["c1_u32_2p20_multi_launch"] = bench_small(ts, torch, ctx, "u32", 0, 20, max(10, args.steps), 5,
+                                                     0x1234 + rank)
+        ctx.set_single_launch(True)
         bd["tiny_slices_u32"] = bench_tiny(ts, torch, ctx, max(10, args.steps))
         bd["c3_by_key_zipf_u64_2p27"] = bench_by_key(ts, torch, ctx, 27, max(3, args.steps // 2), 3, peak)
         for kind in ("u32", "f32"):
