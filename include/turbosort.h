@@ -195,7 +195,7 @@ TS_DECLARE_SEGMENTS(f64, double)
 /* The on-chip method of each segment length bin (32,256] (256,1024]
  * (1024,4096] (4096,16384 or 8192], per key width: 0 bitonic network, 1 radix with
  * 4-bit digits, 2 radix with 8-bit digits, 3 one MSD pass over the key range
- * in shared memory then insertion sorts of the short sub-range runs, 4 (first
+ * in shared memory then each key ranked inside its short sub-range, 4 (first
  * bin only) one warp a segment, eight keys a lane in registers, 5 (second bin,
  * keys of up to 4 bytes) one warp a segment, 16 or 32 keys a lane, 6 (third and
  * fourth bins, keys of 4 and 8 bytes) the MSD pass by thread groups, four or

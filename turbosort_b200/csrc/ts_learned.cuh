@@ -484,14 +484,10 @@ __device__ __forceinline__ LmView lm_load(unsigned char* sm, int L, const LmTabl
     return LmView{leaf, rootk, bp, c};
 }
 
+// Bucket of a key in leaf j (the root search already done): the leaf's
+// piecewise-linear CDF, clamped into the piece's and the leaf's bucket range.
 template <typename U>
-__device__ __forceinline__ int lm_bucket(const LmHead& hd, const LmView& V, int depth, U key) {
-    if (!hd.use_model) {
-        const unsigned long long k = (unsigned long long)key;
-        const float x = k <= hd.kmin ? 0.f : k >= hd.kmax ? 1.f : __ull2float_rn(k - hd.kmin) * hd.inv_range;
-        return min(hd.buckets - 1, (int)(x * (float)hd.buckets));
-    }
-    const int j = lm_root(V.rootk, hd.leaves, depth, lm_prefix(hd, key));
+__device__ __forceinline__ int lm_leaf_bucket(const LmView& V, int j, U key) {
     const LmLeaf lf = V.leaf[j];
     const float t = lm_t(key, lf.klo, lf.winv);
     int k;
@@ -501,6 +497,36 @@ __device__ __forceinline__ int lm_bucket(const LmHead& hd, const LmView& V, int 
     const float c0 = c[k], c1 = c[k + 1];
     const int b = (int)fmaf(c1 - c0, frac, c0);
     return min(max(min(max(b, (int)c0), (int)c1), (int)lf.lo), (int)lf.hi);
+}
+
+// Buckets of N keys at once. The root searches run level by level over all
+// N keys, so each level's N shared reads are independent and overlap (one
+// key's search alone is a chain of `depth` dependent reads).
+template <typename U, int N>
+__device__ __forceinline__ void lm_buckets(const LmHead& hd, const LmView& V, int depth, const U (&key)[N],
+                                           int (&b)[N]) {
+    if (!hd.use_model) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) {
+            const unsigned long long k = (unsigned long long)key[e];
+            const float x = k <= hd.kmin ? 0.f : k >= hd.kmax ? 1.f : __ull2float_rn(k - hd.kmin) * hd.inv_range;
+            b[e] = min(hd.buckets - 1, (int)(x * (float)hd.buckets));
+        }
+        return;
+    }
+    uint32_t p[N];
+    int node[N];
+#pragma unroll
+    for (int e = 0; e < N; ++e) {
+        p[e] = lm_prefix(hd, key[e]);
+        node[e] = 1;
+    }
+    for (int s = 0; s < depth; ++s) {
+#pragma unroll
+        for (int e = 0; e < N; ++e) node[e] = 2 * node[e] + (V.rootk[node[e]] <= p[e] ? 1 : 0);
+    }
+#pragma unroll
+    for (int e = 0; e < N; ++e) b[e] = lm_leaf_bucket<U>(V, min(node[e] - (1 << depth), hd.leaves - 1), key[e]);
 }
 
 constexpr int LM_ILP = 4;
@@ -525,13 +551,17 @@ __global__ void __launch_bounds__(1024) k_lm_count(const U* __restrict__ src, si
             const size_t i = base + (size_t)e * blockDim.x;
             k[e] = i < n ? src[i] : (U)0;
         }
+        U key[LM_ILP];
+#pragma unroll
+        for (int e = 0; e < LM_ILP; ++e) key[e] = to_key<U, XF>(k[e]);
+        int bk[LM_ILP];
+        lm_buckets<U, LM_ILP>(hd, V, depth, key, bk);
 #pragma unroll
         for (int e = 0; e < LM_ILP; ++e) {
             const size_t i = base + (size_t)e * blockDim.x;
             if (i < n) {
-                const int b = lm_bucket(hd, V, depth, to_key<U, XF>(k[e]));
-                ids[i] = (unsigned short)b;
-                atomicAdd(&hist[b], 1u);
+                ids[i] = (unsigned short)bk[e];
+                atomicAdd(&hist[bk[e]], 1u);
             }
         }
     }
